@@ -1,0 +1,222 @@
+// ctx.cu -- device contexts and device-resident instances.
+#include <algorithm>
+#include <cstring>
+
+#include "device.cuh"
+
+extern "C" const unsigned char tamc_expf_blob_begin[];
+extern "C" const unsigned char tamc_expf_blob_end[];
+
+namespace tamc {
+
+static inline uint64_t sm64(uint64_t& st) {
+  st += 0x9e3779b97f4a7c15ULL;
+  uint64_t z = st;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+Xo xo_seed_from_u64(uint64_t seed) {
+  uint64_t st = seed;
+  Xo x;
+  x.s0 = sm64(st);
+  x.s1 = sm64(st);
+  x.s2 = sm64(st);
+  x.s3 = sm64(st);
+  if (!(x.s0 | x.s1 | x.s2 | x.s3)) return xo_seed_from_u64(0);
+  return x;
+}
+
+void xo_jump(Xo& x) {
+  static const uint64_t J[4] = {0x180ec6d33cfd0abaULL, 0xd5a61266f0c9392cULL, 0xa9582618e03fc9aaULL,
+                                0x39abdc4529b1661cULL};
+  uint64_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+  for (int i = 0; i < 4; ++i)
+    for (int b = 0; b < 64; ++b) {
+      if (J[i] & (1ULL << b)) {
+        t0 ^= x.s0;
+        t1 ^= x.s1;
+        t2 ^= x.s2;
+        t3 ^= x.s3;
+      }
+      x.next();
+    }
+  x.s0 = t0;
+  x.s1 = t1;
+  x.s2 = t2;
+  x.s3 = t3;
+}
+
+template <class T>
+static T* dmalloc_copy(const T* h, size_t count) {
+  T* d = nullptr;
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  TAMC_CUDA(cudaMalloc((void**)&d, bytes));
+  if (count) TAMC_CUDA(cudaMemcpy(d, h, count * sizeof(T), cudaMemcpyHostToDevice));
+  return d;
+}
+
+}  // namespace tamc
+
+using namespace tamc;
+
+extern "C" {
+
+int tamc_gpu_open(int device, tamc_gpu** out) {
+  TAMC_API_BEGIN
+  if (!out) fail(TAMC_E_INVAL, "null output");
+  int ndev = 0;
+  TAMC_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) fail(TAMC_E_INVAL, "no such CUDA device");
+  TAMC_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  TAMC_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) fail(TAMC_E_UNSUPPORTED, "this library is built for sm_100a (B200)");
+  auto* g = new tamc_gpu();
+  g->device = device;
+  g->num_sms = prop.multiProcessorCount;
+  g->smem_optin = prop.sharedMemPerBlockOptin;
+  try {
+    TAMC_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    const size_t blob = (size_t)(tamc_expf_blob_end - tamc_expf_blob_begin);
+    uint32_t hdr[3];
+    if (blob < 12) fail(TAMC_E_INVAL, "expf table missing from the library");
+    memcpy(hdr, tamc_expf_blob_begin, 12);
+    if (hdr[0] != 0x54505845u || hdr[1] != TAMC_EXPF_NUM_BUCKETS ||
+        blob != 12 + 4 * ((size_t)hdr[1] + 1 + 2 * (size_t)hdr[2]))
+      fail(TAMC_E_INVAL, "corrupt expf table in the library");
+    g->d_exp = dmalloc_copy((const uint32_t*)(tamc_expf_blob_begin + 12), (blob - 12) / 4);
+    g->exp.off = g->d_exp;
+    g->exp.keys = g->d_exp + hdr[1] + 1;
+    g->exp.vals = g->exp.keys + hdr[2];
+  } catch (...) {
+    if (g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    throw;
+  }
+  *out = g;
+  TAMC_API_END
+}
+
+int tamc_gpu_close(tamc_gpu* g) {
+  TAMC_API_BEGIN
+  if (!g) return TAMC_OK;
+  cudaSetDevice(g->device);
+  cudaStreamSynchronize(g->stream);
+  cudaFree(g->d_exp);
+  cudaStreamDestroy(g->stream);
+  delete g;
+  TAMC_API_END
+}
+
+int tamc_gpu_sync(tamc_gpu* g) {
+  TAMC_API_BEGIN
+  if (!g) fail(TAMC_E_INVAL, "null context");
+  TAMC_CUDA(cudaStreamSynchronize(g->stream));
+  TAMC_API_END
+}
+
+float tamc_ref_expf(float x) {
+  const uint32_t* blob = (const uint32_t*)tamc_expf_blob_begin;
+  const uint32_t nb = blob[1], ne = blob[2];
+  const uint32_t* off = blob + 3;
+  return tamc_expf_exact(x, off, off + nb + 1, off + nb + 1 + ne);
+}
+
+void* tamc_gpu_stream(tamc_gpu* g) { return g ? (void*)g->stream : nullptr; }
+uint64_t tamc_gpu_launch_count(tamc_gpu* g) { return g ? g->launches.load() : 0; }
+
+int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_inst** out) {
+  TAMC_API_BEGIN
+  if (!g || !hi || !out) fail(TAMC_E_INVAL, "null argument");
+  TAMC_CUDA(cudaSetDevice(g->device));
+  const HostInstance& h = hi->h;
+  auto* d = new tamc_inst();
+  d->g = g;
+  d->host = h;
+  d->n = h.n;
+  d->nnz = h.col.size();
+  d->offset = h.offset;
+  d->nchi = (uint32_t)h.suscept.size();
+  d->self_loops = h.has_self_loops();
+  for (uint32_t i = 0; i < h.n; ++i) d->max_deg = std::max(d->max_deg, h.row_ptr[i + 1] - h.row_ptr[i]);
+  try {
+    d->d_rp = dmalloc_copy(h.row_ptr.data(), h.row_ptr.size());
+    d->d_col = dmalloc_copy(h.col.data(), h.col.size());
+    d->d_J = dmalloc_copy(h.J.data(), h.J.size());
+    d->d_bias = dmalloc_copy(h.bias.data(), h.bias.size());
+    // ICM graph: off-diagonal entries over the petgraph node range
+    d->g_nodes = h.graph_nodes();
+    std::vector<uint32_t> grp(d->g_nodes + 1, 0), gcol;
+    for (uint32_t i = 0; i < d->g_nodes; ++i) {
+      for (uint32_t e = h.row_ptr[i]; e < h.row_ptr[i + 1]; ++e)
+        if (h.col[e] != i) gcol.push_back(h.col[e]);
+      grp[i + 1] = (uint32_t)gcol.size();
+    }
+    d->d_grp = dmalloc_copy(grp.data(), grp.size());
+    d->d_gcol = dmalloc_copy(gcol.data(), gcol.size());
+    std::vector<double> sus((size_t)d->nchi * h.n);
+    for (uint32_t k = 0; k < d->nchi; ++k) std::copy(h.suscept[k].begin(), h.suscept[k].end(), sus.begin() + (size_t)k * h.n);
+    d->d_sus = dmalloc_copy(sus.data(), sus.size());
+    // colour order
+    std::vector<uint32_t> color;
+    h.coloring(d->ncolors, color);
+    if (h.n == 0) d->ncolors = 0;
+    d->color_off.assign(d->ncolors + 1, 0);
+    for (uint32_t i = 0; i < h.n; ++i) d->color_off[color[i] + 1]++;
+    for (uint32_t c = 0; c < d->ncolors; ++c) d->color_off[c + 1] += d->color_off[c];
+    std::vector<uint32_t> fill(d->color_off.begin(), d->color_off.end() - (d->ncolors ? 1 : 0));
+    d->h_perm.assign(h.n, 0);
+    std::vector<uint32_t> iperm(h.n);
+    for (uint32_t i = 0; i < h.n; ++i) {
+      const uint32_t s = fill[color[i]]++;
+      d->h_perm[s] = i;
+      iperm[i] = s;
+    }
+    std::vector<uint32_t> frp(h.n + 1, 0);
+    std::vector<uint2> fent;
+    fent.reserve(h.col.size());
+    std::vector<float> fbias(h.n), fkd(h.n, 0.0f);
+    std::vector<double> fsus((size_t)d->nchi * h.n);
+    for (uint32_t s = 0; s < h.n; ++s) {
+      const uint32_t i = d->h_perm[s];
+      fbias[s] = h.bias[i];
+      for (uint32_t e = h.row_ptr[i]; e < h.row_ptr[i + 1]; ++e) {
+        uint32_t jb;
+        memcpy(&jb, &h.J[e], 4);
+        fent.push_back(make_uint2(iperm[h.col[e]], jb));
+        if (h.col[e] == i) fkd[s] += h.J[e];
+      }
+      frp[s + 1] = (uint32_t)fent.size();
+      for (uint32_t k = 0; k < d->nchi; ++k) fsus[(size_t)k * h.n + s] = h.suscept[k][i];
+    }
+    d->d_color_off = dmalloc_copy(d->color_off.data(), d->color_off.size());
+    d->d_perm = dmalloc_copy(d->h_perm.data(), d->h_perm.size());
+    d->d_iperm = dmalloc_copy(iperm.data(), iperm.size());
+    d->d_frp = dmalloc_copy(frp.data(), frp.size());
+    d->d_fent = dmalloc_copy(fent.data(), fent.size());
+    d->d_fbias = dmalloc_copy(fbias.data(), fbias.size());
+    d->d_fkd = dmalloc_copy(fkd.data(), fkd.size());
+    d->d_fsus = dmalloc_copy(fsus.data(), fsus.size());
+  } catch (...) {
+    tamc_gpu_instance_destroy(d);
+    throw;
+  }
+  *out = d;
+  TAMC_API_END
+}
+
+int tamc_gpu_instance_destroy(tamc_inst* d) {
+  TAMC_API_BEGIN
+  if (!d) return TAMC_OK;
+  cudaSetDevice(d->g->device);
+  void* ptrs[] = {d->d_rp, d->d_col, d->d_J, d->d_bias, d->d_grp, d->d_gcol, d->d_sus, d->d_color_off,
+                  d->d_perm, d->d_iperm, d->d_frp, d->d_fent, d->d_fbias, d->d_fkd, d->d_fsus};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete d;
+  TAMC_API_END
+}
+
+}  // extern "C"

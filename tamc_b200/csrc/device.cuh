@@ -1,0 +1,144 @@
+// device.cuh -- device-side building blocks shared by every kernel file.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "expf_exact.h"
+#include "internal.h"
+
+namespace tamc {
+
+#define TAMC_CUDA(call)                                                                  \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      ::tamc::fail(TAMC_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+// ------------------------------------------------------------ RNG ----
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of the
+// multiply-hi/lo Feistel round with multipliers 0xD2511F53 / 0xCD9E8D57 and
+// Weyl key increments 0x9E3779B9 / 0xBB67AE85.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// Counter tags that keep the Philox streams of different uses disjoint.
+enum : uint32_t {
+  PTAG_SWEEP = 0x5357u,   // Metropolis uniforms
+  PTAG_INIT = 0x494eu,    // initial spins
+  PTAG_ICM = 0x4943u,     // ICM seed-site choice
+  PTAG_EXCH = 0x4558u,    // replica-exchange uniforms
+};
+
+__host__ __device__ __forceinline__ uint2 philox_key(uint64_t seed) {
+  return make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+// Xoshiro256++ (Blackman & Vigna 2018) as used by the reference through
+// rand_xoshiro::Xoshiro256PlusPlus; next_u32 = upper half (rand_xoshiro).
+struct Xo {
+  uint64_t s0, s1, s2, s3;
+  __host__ __device__ __forceinline__ uint64_t next() {
+    const uint64_t r = ((s0 + s3) << 23 | (s0 + s3) >> 41) + s0;
+    const uint64_t t = s1 << 17;
+    s2 ^= s0;
+    s3 ^= s1;
+    s1 ^= s2;
+    s0 ^= s3;
+    s2 ^= t;
+    s3 = (s3 << 45) | (s3 >> 19);
+    return r;
+  }
+  __host__ __device__ __forceinline__ uint32_t next_u32() { return (uint32_t)(next() >> 32); }
+  // rand 0.8 `Standard` f32: 24 random bits times 2^-24.
+  __host__ __device__ __forceinline__ float std_f32() { return (float)(next_u32() >> 8) * (1.0f / 16777216.0f); }
+  // rand 0.8 UniformInt<u32>::sample_single over [0, range), range > 0.
+  __host__ __device__ __forceinline__ uint32_t gen_range(uint32_t range) {
+#if defined(__CUDA_ARCH__)
+    const uint32_t zone = (range << __clz(range)) - 1u;
+#else
+    const uint32_t zone = (range << __builtin_clz(range)) - 1u;
+#endif
+    for (;;) {
+      const uint32_t v = next_u32();
+      const uint64_t m = (uint64_t)v * (uint64_t)range;
+      if ((uint32_t)m <= zone) return (uint32_t)(m >> 32);
+    }
+  }
+};
+
+// Host-side seeding (rand_xoshiro seed_from_u64 = SplitMix64 fill) and jump.
+Xo xo_seed_from_u64(uint64_t seed);
+void xo_jump(Xo& x);
+
+// ------------------------------------------------------- contexts ----
+struct ExpTable {
+  const uint32_t* off;
+  const uint32_t* keys;
+  const uint32_t* vals;
+};
+
+}  // namespace tamc
+
+struct tamc_gpu {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  size_t smem_optin = 0;
+  uint32_t* d_exp = nullptr;  // exception table blob
+  tamc::ExpTable exp{};
+  std::atomic<uint64_t> launches{0};
+  void count(uint64_t k = 1) { launches.fetch_add(k, std::memory_order_relaxed); }
+};
+
+// Device-resident instance.  Two site orders are kept:
+//  * reference order (row i = site i, entries sorted by column, self-loops
+//    included) for the reference-order kernels and the ICM graph;
+//  * colour order for the fast kernels: sites of colour class 0 first, then
+//    class 1, ...; fent[e] = (new column index, J bits) in the reference's
+//    per-row order so ΔE is summed in the same order as the reference.
+struct tamc_inst {
+  tamc_gpu* g = nullptr;
+  uint32_t n = 0;
+  uint64_t nnz = 0;
+  float offset = 0.0f;
+  uint32_t nchi = 0;
+  bool self_loops = false;
+  uint32_t max_deg = 0;
+  // reference order
+  uint32_t* d_rp = nullptr;
+  uint32_t* d_col = nullptr;
+  float* d_J = nullptr;
+  float* d_bias = nullptr;
+  uint32_t g_nodes = 0;
+  uint32_t* d_grp = nullptr;   // ICM graph rows (petgraph node range), off-diagonal
+  uint32_t* d_gcol = nullptr;
+  double* d_sus = nullptr;     // [nchi][n] reference order
+  // colour order
+  uint32_t ncolors = 0;
+  std::vector<uint32_t> color_off;   // host copy, ncolors + 1
+  uint32_t* d_color_off = nullptr;
+  uint32_t* d_perm = nullptr;        // new -> original
+  uint32_t* d_iperm = nullptr;       // original -> new
+  uint32_t* d_frp = nullptr;         // n + 1
+  uint2* d_fent = nullptr;           // nnz (col_new, J bits)
+  float* d_fbias = nullptr;          // n
+  float* d_fkd = nullptr;            // n: self-loop coefficient (0 if none)
+  double* d_fsus = nullptr;          // [nchi][n] colour order
+  // host copies used by drivers
+  tamc::HostInstance host;
+  std::vector<uint32_t> h_perm;
+};

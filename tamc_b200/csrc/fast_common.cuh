@@ -1,0 +1,116 @@
+// fast_common.cuh -- building blocks of the colour-ordered (TAMC_MODE_FAST) kernels.
+//
+// Spin storage is bit-sliced across replicas: for every site a 32-bit word
+// whose bit b is the spin of replica b of the word's group (1 = spin -1, the
+// reference's packing convention, src/ising.rs:102-115).  A "quad" is 4
+// adjacent bits; one task updates one site for the 4 replicas of a quad, with
+// the 4 uniforms of one Philox-4x32-10 call keyed by (seed) and countered by
+// (site, sweep, quad id, tag), so results do not depend on how tasks are
+// spread over threads or CTAs.
+#pragma once
+#include "device.cuh"
+
+namespace tamc {
+
+struct FastInst {  // colour-ordered instance (device pointers)
+  uint32_t n, nnz, ncolors;
+  float offset;
+  const uint32_t* color_off;  // ncolors + 1
+  const uint32_t* perm;       // new -> original
+  const uint32_t* iperm;      // original -> new
+  const uint32_t* rp;         // n + 1
+  const uint2* ent;           // nnz (new column, J bits)
+  const float* bias;          // n
+  const float* kd;            // n self-loop coefficient
+  const double* sus;          // [nchi][n], colour order
+  uint32_t nchi;
+};
+
+FastInst make_fast_inst(const tamc_inst* d);
+
+// Local field of site s for the 4 replicas held in bits [shift, shift+4) of
+// the words W[j * ws + wo]:  f_r = h_s + Σ_j J_sj s_j^r, summed in the
+// reference's row order (src/ising.rs:471-475).
+__device__ __forceinline__ float4 local_field4(uint32_t s, uint32_t shift, const uint32_t* __restrict__ rp,
+                                               const uint2* __restrict__ ent, const float* __restrict__ bias,
+                                               const uint32_t* W, uint32_t ws, uint32_t wo) {
+  const uint32_t e0 = rp[s], e1 = rp[s + 1];
+  const float h = bias[s];
+  float4 f = make_float4(h, h, h, h);
+  for (uint32_t e = e0; e < e1; ++e) {
+    const uint2 c = ent[e];
+    const uint32_t w = W[c.x * ws + wo] >> shift;
+    f.x += __uint_as_float(c.y ^ (w << 31));
+    f.y += __uint_as_float(c.y ^ ((w << 30) & 0x80000000u));
+    f.z += __uint_as_float(c.y ^ ((w << 29) & 0x80000000u));
+    f.w += __uint_as_float(c.y ^ ((w << 28) & 0x80000000u));
+  }
+  return f;
+}
+
+// ΔE_r = -2 s_r f_r for the quad (src/ising.rs:476-477).
+__device__ __forceinline__ float4 delta4(float4 f, uint32_t own) {
+  float4 d;
+  d.x = __uint_as_float(__float_as_uint(-2.0f * f.x) ^ (own << 31));
+  d.y = __uint_as_float(__float_as_uint(-2.0f * f.y) ^ ((own << 30) & 0x80000000u));
+  d.z = __uint_as_float(__float_as_uint(-2.0f * f.z) ^ ((own << 29) & 0x80000000u));
+  d.w = __uint_as_float(__float_as_uint(-2.0f * f.w) ^ ((own << 28) & 0x80000000u));
+  return d;
+}
+
+// Metropolis rule: accept iff u < exp(-beta * max(ΔE, 0)) with u a 24-bit
+// uniform; ΔE <= 0 always accepts (p = 1), as the reference's rule does.
+__device__ __forceinline__ bool accept1(float dE, float beta, uint32_t r) {
+  const float p = __expf(-beta * fmaxf(dE, 0.0f));
+  return (float)(r >> 8) * (1.0f / 16777216.0f) < p;
+}
+
+// One quad update.  Returns the 4-bit flip mask; adds accepted ΔE to acc.
+__device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
+                                                uint32_t ws, uint32_t wo, float4 beta, uint4 rnd, float4& acc) {
+  const float4 f = local_field4(s, shift, F.rp, F.ent, F.bias, W, ws, wo);
+  const uint32_t own = W[s * ws + wo] >> shift;
+  const float4 d = delta4(f, own);
+  const bool a0 = accept1(d.x, beta.x, rnd.x);
+  const bool a1 = accept1(d.y, beta.y, rnd.y);
+  const bool a2 = accept1(d.z, beta.z, rnd.z);
+  const bool a3 = accept1(d.w, beta.w, rnd.w);
+  acc.x += a0 ? d.x : 0.0f;
+  acc.y += a1 ? d.y : 0.0f;
+  acc.z += a2 ? d.z : 0.0f;
+  acc.w += a3 ? d.w : 0.0f;
+  return (uint32_t)a0 | ((uint32_t)a1 << 1) | ((uint32_t)a2 << 2) | ((uint32_t)a3 << 3);
+}
+
+// Per-replica energy contribution of site s for a quad:
+//   e_r = s_r (h_s + Σ_j J_sj s_j^r / 2)   (energy_ref row term, src/ising.rs:441-449)
+__device__ __forceinline__ float4 energy_terms4(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
+                                                uint32_t ws, uint32_t wo) {
+  const uint32_t e0 = F.rp[s], e1 = F.rp[s + 1];
+  const float h = F.bias[s];
+  float4 f = make_float4(h, h, h, h);
+  for (uint32_t e = e0; e < e1; ++e) {
+    const uint2 c = F.ent[e];
+    const uint32_t w = W[c.x * ws + wo] >> shift;
+    const uint32_t hj = __float_as_uint(0.5f * __uint_as_float(c.y));
+    f.x += __uint_as_float(hj ^ (w << 31));
+    f.y += __uint_as_float(hj ^ ((w << 30) & 0x80000000u));
+    f.z += __uint_as_float(hj ^ ((w << 29) & 0x80000000u));
+    f.w += __uint_as_float(hj ^ ((w << 28) & 0x80000000u));
+  }
+  const uint32_t own = W[s * ws + wo] >> shift;
+  float4 e;
+  e.x = __uint_as_float(__float_as_uint(f.x) ^ (own << 31));
+  e.y = __uint_as_float(__float_as_uint(f.y) ^ ((own << 30) & 0x80000000u));
+  e.z = __uint_as_float(__float_as_uint(f.z) ^ ((own << 29) & 0x80000000u));
+  e.w = __uint_as_float(__float_as_uint(f.w) ^ ((own << 28) & 0x80000000u));
+  return e;
+}
+
+// 4 initial spins from one Philox call: spin = +1 iff the top bit is set
+// (the same rule as rand_ising_state's Uniform(0,1), src/ising.rs:172).
+__device__ __forceinline__ uint32_t init_nibble(uint4 r) {
+  return (r.x >> 31 ^ 1u) | ((r.y >> 31 ^ 1u) << 1) | ((r.z >> 31 ^ 1u) << 2) | ((r.w >> 31 ^ 1u) << 3);
+}
+
+}  // namespace tamc

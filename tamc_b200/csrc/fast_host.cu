@@ -1,0 +1,524 @@
+// fast_host.cu -- host side of the colour-ordered PT-ICM path: the tamc_pt
+// glue (one job), the batched runner (many jobs per launch, each chunk of
+// rounds replayed from a captured CUDA graph) and the tile autotuner.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "fast_pt.cuh"
+
+struct tamc_pt::FastState {
+  tamc::PtJob job{};
+  tamc::DBuf<uint32_t> W;
+  tamc::DBuf<double> Ec, Er;
+  tamc::DBuf<uint8_t> tags;
+  tamc::DBuf<uint32_t> acc, rtrips, dhist;
+  tamc::DBuf<float> betas;
+  tamc::DBuf<tamc::PtJob> d_job;
+  tamc::DBuf<uint32_t> ctr;
+  uint32_t T = 512;
+  size_t smem = 0;
+};
+
+namespace tamc {
+
+// ------------------------------------------------------------ autotuner ----
+// The fused kernel's free choices per job shape are the CTA size and whether
+// the colour-ordered CSR is staged in shared memory.  Candidates are timed on a
+// scratch copy of the job (a few rounds, CUDA events) the first time a shape
+// is seen; the winner is cached per (device, n, nnz, nt, C) shape.
+struct TileChoice {
+  uint32_t T;
+  bool csr;
+};
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t, int>, TileChoice> g_tune;
+
+static bool fits(const tamc_gpu* g, const PtJob& j, uint32_t T, bool csr) {
+  return fused_smem_bytes(j, T, csr) <= g->smem_optin;
+}
+
+static TileChoice heuristic_tile(const tamc_gpu* g, const PtJob& j) {
+  TileChoice t{512, true};
+  if (!fits(g, j, t.T, true)) t.csr = false;
+  return t;
+}
+
+static float time_tile(tamc_gpu* g, const PtJob& proto, TileChoice t, uint32_t rounds) {
+  // scratch state so the real job is untouched
+  PtJob j = proto;
+  DBuf<uint32_t> W((size_t)j.n * j.nw);
+  DBuf<double> Ec((size_t)j.C * j.ntp), Er((size_t)j.C * j.ntp);
+  DBuf<uint8_t> tags((size_t)j.C * j.nt);
+  DBuf<uint32_t> acc((size_t)j.C * j.nt), rt(j.C), dh((size_t)j.C * j.nt * 2);
+  DBuf<PtJob> dj(1);
+  DBuf<uint32_t> ctr(1);
+  cudaStream_t st = g->stream;
+  tags.zero(st);
+  acc.zero(st);
+  rt.zero(st);
+  dh.zero(st);
+  j.W = W.p;
+  j.Ec = Ec.p;
+  j.Er = Er.p;
+  j.tags = tags.p;
+  j.acc = acc.p;
+  j.rtrips = rt.p;
+  j.dhist = dh.p;
+  j.init = 1;
+  j.sweep_begin = 0;
+  j.sweep_end = rounds;
+  j.meas_init = 0xffffffffu;  // no measurements while timing
+  j.count_out = nullptr;
+  j.csr_smem = t.csr;
+  TAMC_CUDA(cudaMemcpyAsync(dj.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
+  const size_t smem = fused_smem_bytes(j, t.T, t.csr);
+  cudaEvent_t e0, e1;
+  TAMC_CUDA(cudaEventCreate(&e0));
+  TAMC_CUDA(cudaEventCreate(&e1));
+  float ms = 0.0f;
+  for (int rep = 0; rep < 2; ++rep) {  // first run warms up
+    ctr.zero(st);
+    TAMC_CUDA(cudaEventRecord(e0, st));
+    fused_launch(st, dj.p, 1, ctr.p, 1, t.T, smem);
+    TAMC_CUDA(cudaEventRecord(e1, st));
+    g->count();
+  }
+  TAMC_CUDA(cudaEventSynchronize(e1));
+  TAMC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+static TileChoice tune_tile(tamc_gpu* g, const PtJob& j) {
+  const auto key = std::make_tuple(g->device, j.n, j.F.nnz, j.nt, j.C, (int)j.self_loops);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+  }
+  TileChoice best = heuristic_tile(g, j);
+  const char* env = getenv("TAMC_AUTOTUNE");
+  if (!env || env[0] != '0') {
+    float best_ms = 1e30f;
+    for (uint32_t T : {128u, 256u, 512u}) {
+      if (T < j.qps) continue;
+      for (bool csr : {true, false}) {
+        if (!fits(g, j, T, csr)) continue;
+        const float ms = time_tile(g, j, TileChoice{T, csr}, 4);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = TileChoice{T, csr};
+        }
+      }
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+  return best;
+}
+
+// ------------------------------------------------------------ one job ----
+static void fill_job(tamc_pt* pt, uint64_t seed, tamc_pt::FastState* F) {
+  const PtCfg& c = pt->cfg;
+  const tamc_inst* I = pt->inst;
+  if (c.nt > 64) fail(TAMC_E_UNSUPPORTED, "fast mode supports at most 64 temperatures per chain");
+  PtJob& j = F->job;
+  j.F = make_fast_inst(I);
+  j.n = I->n;
+  j.nt = c.nt;
+  j.ntp = (c.nt + 3) & ~3u;
+  j.C = c.C;
+  j.wpc = (j.ntp + 31) / 32;
+  j.nw = j.C * j.wpc;
+  j.lo = c.lo;
+  j.qpc = j.ntp / 4;
+  j.qps = j.C * j.qpc;
+  if (j.qps > 512) fail(TAMC_E_UNSUPPORTED, "fast mode supports at most 2048 replicas per run");
+  j.icm = c.icm;
+  j.threaded = c.threads > 1;
+  j.self_loops = I->self_loops;
+  j.key = philox_key(seed);
+  cudaStream_t st = pt->g->stream;
+  F->W.alloc((size_t)j.n * j.nw);
+  F->Ec.alloc((size_t)j.C * j.ntp);
+  F->Er.alloc((size_t)j.C * j.ntp);
+  F->tags.alloc((size_t)j.C * j.nt);
+  F->acc.alloc((size_t)j.C * j.nt);
+  F->rtrips.alloc(j.C);
+  F->dhist.alloc((size_t)j.C * j.nt * 2);
+  F->betas.alloc(j.ntp);
+  F->d_job.alloc(1);
+  F->ctr.alloc(1);
+  std::vector<float> b(j.ntp, 0.0f);
+  std::copy(c.betas.begin(), c.betas.end(), b.begin());
+  TAMC_CUDA(cudaMemcpyAsync(F->betas.p, b.data(), j.ntp * 4, cudaMemcpyHostToDevice, st));
+  std::vector<uint8_t> tags((size_t)j.C * j.nt, 0);
+  for (uint32_t ch = 0; ch < j.C; ++ch) {
+    tags[(size_t)ch * j.nt] = 1;
+    tags[(size_t)ch * j.nt + j.nt - 1] = 2;
+  }
+  TAMC_CUDA(cudaMemcpyAsync(F->tags.p, tags.data(), tags.size(), cudaMemcpyHostToDevice, st));
+  F->acc.zero(st);
+  F->rtrips.zero(st);
+  F->dhist.zero(st);
+  j.betas = F->betas.p;
+  j.W = F->W.p;
+  j.Ec = F->Ec.p;
+  j.Er = F->Er.p;
+  j.tags = F->tags.p;
+  j.acc = F->acc.p;
+  j.rtrips = F->rtrips.p;
+  j.dhist = F->dhist.p;
+  j.num_sweeps = c.num_sweeps;
+  j.meas_init = c.meas_init;
+  j.sample = c.sample;
+  j.sample_states = c.sample_states;
+  j.level = c.level;
+  j.out = pt->out.meas(c);
+  j.log = pt->out.log();
+  j.count_out = nullptr;
+  j.cost = (uint64_t)c.num_sweeps * j.n * j.C * j.ntp;
+}
+
+static uint32_t count_sched(int64_t period, uint32_t meas_init, uint32_t num_sweeps, uint32_t a, uint32_t b) {
+  uint32_t k = 0;
+  for (uint32_t i = std::max(a, meas_init); i < b; ++i)
+    k += period >= 0 && ((i - meas_init) % (uint32_t)period == 0 || i == num_sweeps - 1);
+  return k;
+}
+
+static void launch_one(tamc_pt* pt, uint32_t begin, uint32_t end, int init) {
+  auto* F = pt->fast;
+  PtJob& j = F->job;
+  cudaStream_t st = pt->g->stream;
+  j.init = init;
+  j.sweep_begin = begin;
+  j.sweep_end = end;
+  j.m_base = pt->m_next;
+  j.s_base = pt->s_next;
+  TAMC_CUDA(cudaMemcpyAsync(F->d_job.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
+  F->ctr.zero(st);
+  fused_launch(st, F->d_job.p, 1, F->ctr.p, 1, F->T, F->smem);
+  pt->g->count();
+  // the job struct is read by the kernel; keep the host copy alive until done
+  TAMC_CUDA(cudaStreamSynchronize(st));
+}
+
+void fast_pt_create(tamc_pt* pt, uint64_t seed) {
+  pt->fast = new tamc_pt::FastState();
+  fill_job(pt, seed, pt->fast);
+  const TileChoice t = tune_tile(pt->g, pt->fast->job);
+  pt->fast->T = t.T;
+  pt->fast->job.csr_smem = t.csr;
+  pt->fast->smem = fused_smem_bytes(pt->fast->job, t.T, t.csr);
+  if (pt->fast->smem > pt->g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the fused PT kernel");
+  launch_one(pt, 0, 0, 1);  // random initial replicas and their energies
+}
+
+void fast_pt_run(tamc_pt* pt, uint32_t sweep_end) {
+  const PtCfg& c = pt->cfg;
+  while (pt->next_sweep < sweep_end) {
+    const uint32_t b = pt->next_sweep;
+    const uint32_t e = std::min(sweep_end, b + pt->out.cap);
+    launch_one(pt, b, e, 0);
+    pt->m_next += count_sched(c.sample, c.meas_init, c.num_sweeps, b, e);
+    pt->s_next += count_sched(c.sample_states, c.meas_init, c.num_sweeps, b, e);
+    pt->next_sweep = e;
+    pt->out.drain(pt->g->stream);
+  }
+}
+
+void fast_pt_get_state(tamc_pt* pt, int8_t* spins, float* energies) {
+  auto* F = pt->fast;
+  const PtJob& j = F->job;
+  cudaStream_t st = pt->g->stream;
+  std::vector<uint32_t> W((size_t)j.n * j.nw);
+  std::vector<double> Ec((size_t)j.C * j.ntp);
+  TAMC_CUDA(cudaMemcpyAsync(W.data(), F->W.p, W.size() * 4, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(cudaMemcpyAsync(Ec.data(), F->Ec.p, Ec.size() * 8, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(cudaStreamSynchronize(st));
+  const std::vector<uint32_t>& perm = pt->inst->h_perm;
+  for (uint32_t ch = 0; ch < j.C; ++ch)
+    for (uint32_t t = 0; t < j.nt; ++t) {
+      if (energies) energies[(size_t)ch * j.nt + t] = (float)Ec[(size_t)ch * j.ntp + t];
+      if (!spins) continue;
+      int8_t* dst = spins + ((size_t)ch * j.nt + t) * j.n;
+      const uint32_t o = ch * j.wpc + t / 32, b = t % 32;
+      for (uint32_t s = 0; s < j.n; ++s) dst[perm[s]] = ((W[(size_t)s * j.nw + o] >> b) & 1u) ? -1 : 1;
+    }
+}
+
+void fast_pt_set_state(tamc_pt* pt, const int8_t* spins) {
+  auto* F = pt->fast;
+  const PtJob& j = F->job;
+  cudaStream_t st = pt->g->stream;
+  std::vector<uint32_t> W((size_t)j.n * j.nw, 0);
+  const std::vector<uint32_t>& perm = pt->inst->h_perm;
+  for (uint32_t ch = 0; ch < j.C; ++ch)
+    for (uint32_t t = 0; t < j.nt; ++t) {
+      const int8_t* src = spins + ((size_t)ch * j.nt + t) * j.n;
+      const uint32_t o = ch * j.wpc + t / 32, b = t % 32;
+      for (uint32_t s = 0; s < j.n; ++s)
+        if (src[perm[s]] < 0) W[(size_t)s * j.nw + o] |= 1u << b;
+    }
+  TAMC_CUDA(cudaMemcpyAsync(F->W.p, W.data(), W.size() * 4, cudaMemcpyHostToDevice, st));
+  launch_one(pt, pt->next_sweep, pt->next_sweep, 2);  // recompute energies
+}
+
+void fast_pt_acceptance(tamc_pt* pt, uint32_t* acc) {
+  auto* F = pt->fast;
+  TAMC_CUDA(cudaMemcpyAsync(acc, F->acc.p, F->acc.n * 4, cudaMemcpyDeviceToHost, pt->g->stream));
+  TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
+}
+
+void fast_pt_round_trips(tamc_pt* pt, uint8_t* tags, uint32_t* round_trips, uint32_t* dhist) {
+  auto* F = pt->fast;
+  cudaStream_t st = pt->g->stream;
+  if (tags) TAMC_CUDA(cudaMemcpyAsync(tags, F->tags.p, F->tags.n, cudaMemcpyDeviceToHost, st));
+  if (round_trips) TAMC_CUDA(cudaMemcpyAsync(round_trips, F->rtrips.p, F->rtrips.n * 4, cudaMemcpyDeviceToHost, st));
+  if (dhist) TAMC_CUDA(cudaMemcpyAsync(dhist, F->dhist.p, F->dhist.n * 4, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(cudaStreamSynchronize(st));
+}
+
+void fast_pt_destroy(tamc_pt* pt) {
+  delete pt->fast;
+  pt->fast = nullptr;
+}
+
+}  // namespace tamc
+
+// ================================================================ batch ====
+namespace tamc {
+
+// Runs one chunk of PT rounds for a set of fast-mode runs in a single fused
+// launch (jobs ordered longest-remaining-first).  With `graph`, the
+// upload -> reset -> kernel -> readback sequence is captured once per job
+// count / tile and replayed for every later chunk.
+struct ChunkRunner {
+  DBuf<PtJob> d_jobs;
+  DBuf<uint32_t> ctr;
+  DBuf<uint32_t> counts;
+  PtJob* h_jobs = nullptr;
+  uint32_t* h_counts = nullptr;
+  uint32_t cap_jobs = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint32_t g_n = 0, g_grid = 0, g_T = 0;
+  size_t g_smem = 0;
+  ~ChunkRunner() { reset(); }
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    if (h_jobs) cudaFreeHost(h_jobs);
+    if (h_counts) cudaFreeHost(h_counts);
+    h_jobs = nullptr;
+    h_counts = nullptr;
+    cap_jobs = 0;
+  }
+  void reserve(uint32_t n) {
+    if (n <= cap_jobs) return;
+    reset();
+    cap_jobs = std::max(n, 16u);
+    TAMC_CUDA(cudaMallocHost((void**)&h_jobs, cap_jobs * sizeof(PtJob)));
+    TAMC_CUDA(cudaMallocHost((void**)&h_counts, cap_jobs * sizeof(uint32_t)));
+    d_jobs.alloc(cap_jobs);
+    ctr.alloc(1);
+    counts.alloc(cap_jobs);
+  }
+  // Advances every run in `act` by up to `chunk` rounds.
+  void run(tamc_gpu* g, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph) {
+    cudaStream_t st = g->stream;
+    act.erase(std::remove_if(act.begin(), act.end(),
+                             [](tamc_pt* p) { return p->next_sweep >= p->cfg.num_sweeps; }),
+              act.end());
+    if (act.empty()) return;
+    auto remaining = [](const tamc_pt* p) {
+      return (uint64_t)(p->cfg.num_sweeps - p->next_sweep) * (p->fast->job.cost / std::max(1u, p->cfg.num_sweeps));
+    };
+    std::stable_sort(act.begin(), act.end(), [&](tamc_pt* x, tamc_pt* y) { return remaining(x) > remaining(y); });
+    // one CTA size per launch: the autotuned size of the costliest run
+    uint32_t T = act[0]->fast->T;
+    for (auto* pt : act)
+      if (T < pt->fast->job.qps) T = 512;
+    size_t smem = 0;
+    for (auto* pt : act) {
+      PtJob& j = pt->fast->job;
+      if (fused_smem_bytes(j, T, j.csr_smem) > g->smem_optin) j.csr_smem = 0;
+      smem = std::max(smem, fused_smem_bytes(j, T, j.csr_smem));
+    }
+    if (smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "a run is too large for the fused PT kernel");
+    const uint32_t na = (uint32_t)act.size();
+    reserve(na);
+    std::vector<uint32_t> ends(na);
+    for (uint32_t x = 0; x < na; ++x) {
+      tamc_pt* pt = act[x];
+      PtJob j = pt->fast->job;
+      j.init = 0;
+      j.sweep_begin = pt->next_sweep;
+      ends[x] = std::min(pt->cfg.num_sweeps, pt->next_sweep + std::min(chunk, pt->out.cap));
+      j.sweep_end = ends[x];
+      j.m_base = pt->m_next;
+      j.s_base = pt->s_next;
+      j.count_out = counts.p + x;
+      h_jobs[x] = j;
+    }
+    const int per_sm = fused_blocks_per_sm(T, smem);
+    const uint32_t grid = std::min<uint32_t>(na, (uint32_t)(g->num_sms * std::max(per_sm, 1)));
+    if (use_graph) {
+      if (!exec || g_n != na || g_grid != grid || g_T != T || g_smem != smem) {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        TAMC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaMemcpyAsync(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(ctr.p, 0, 4, st);
+        fused_launch(st, d_jobs.p, na, ctr.p, grid, T, smem);
+        cudaMemcpyAsync(h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st);
+        TAMC_CUDA(cudaStreamEndCapture(st, &graph));
+        TAMC_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        g_n = na;
+        g_grid = grid;
+        g_T = T;
+        g_smem = smem;
+      }
+      TAMC_CUDA(cudaGraphLaunch(exec, st));
+    } else {
+      TAMC_CUDA(cudaMemcpyAsync(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st));
+      TAMC_CUDA(cudaMemsetAsync(ctr.p, 0, 4, st));
+      fused_launch(st, d_jobs.p, na, ctr.p, grid, T, smem);
+      TAMC_CUDA(cudaMemcpyAsync(h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st));
+    }
+    g->count();
+    TAMC_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t x = 0; x < na; ++x) {
+      tamc_pt* pt = act[x];
+      const PtCfg& c = pt->cfg;
+      pt->m_next += count_sched(c.sample, c.meas_init, c.num_sweeps, pt->next_sweep, ends[x]);
+      pt->s_next += count_sched(c.sample_states, c.meas_init, c.num_sweeps, pt->next_sweep, ends[x]);
+      pt->next_sweep = ends[x];
+      if (h_counts[x]) pt->out.drain(st);
+      else pt->out.pending = 0;
+    }
+  }
+};
+
+void chunk_run(ChunkRunner* r, tamc_gpu* g, std::vector<tamc_pt*>& act, uint32_t chunk) {
+  r->run(g, act, chunk, false);
+}
+ChunkRunner* chunk_runner_new() { return new ChunkRunner(); }
+void chunk_runner_free(ChunkRunner* r) { delete r; }
+
+}  // namespace tamc
+
+using namespace tamc;
+
+struct tamc_batch {
+  tamc_gpu* g = nullptr;
+  std::vector<tamc_pt*> jobs;
+  ChunkRunner runner;
+  uint32_t chunk = 256;
+  ~tamc_batch() {
+    runner.reset();
+    for (auto* p : jobs) tamc_gpu_pt_destroy(p);
+  }
+};
+
+extern "C" {
+
+int tamc_gpu_batch_create(tamc_gpu* g, tamc_batch** out) {
+  TAMC_API_BEGIN
+  if (!g || !out) fail(TAMC_E_INVAL, "null argument");
+  auto* b = new tamc_batch();
+  b->g = g;
+  *out = b;
+  TAMC_API_END
+}
+
+int tamc_gpu_batch_add(tamc_batch* b, tamc_inst* inst, const tamc_pt_params* p, uint64_t seed, uint32_t* job) {
+  TAMC_API_BEGIN
+  if (!b || !inst) fail(TAMC_E_INVAL, "null argument");
+  tamc_pt* pt = nullptr;
+  const int rc = tamc_gpu_pt_create(inst, p, seed, TAMC_MODE_FAST, &pt);
+  if (rc != TAMC_OK) return rc;
+  b->jobs.push_back(pt);
+  if (job) *job = (uint32_t)(b->jobs.size() - 1);
+  TAMC_API_END
+}
+
+int tamc_gpu_batch_run(tamc_batch* b) {
+  TAMC_API_BEGIN
+  if (!b) fail(TAMC_E_INVAL, "null batch");
+  TAMC_CUDA(cudaSetDevice(b->g->device));
+  for (;;) {
+    bool any = false;
+    for (auto* pt : b->jobs) any |= pt->next_sweep < pt->cfg.num_sweeps;
+    if (!any) break;
+    b->runner.run(b->g, b->jobs, b->chunk, true);
+  }
+  TAMC_API_END
+}
+
+int tamc_gpu_batch_sync(tamc_batch* b) {
+  TAMC_API_BEGIN
+  if (!b) fail(TAMC_E_INVAL, "null batch");
+  TAMC_CUDA(cudaStreamSynchronize(b->g->stream));
+  TAMC_API_END
+}
+
+static tamc_pt* job_of(tamc_batch* b, uint32_t job) {
+  if (!b || job >= b->jobs.size()) fail(TAMC_E_INVAL, "no such job");
+  return b->jobs[job];
+}
+
+int tamc_gpu_batch_get_state(tamc_batch* b, uint32_t job, int8_t* spins, float* energies) {
+  TAMC_API_BEGIN
+  return tamc_gpu_pt_get_state(job_of(b, job), spins, energies);
+  TAMC_API_END
+}
+int tamc_gpu_batch_acceptance(tamc_batch* b, uint32_t job, uint32_t* counts) {
+  TAMC_API_BEGIN
+  return tamc_gpu_pt_acceptance(job_of(b, job), counts);
+  TAMC_API_END
+}
+int tamc_gpu_batch_gs(tamc_batch* b, uint32_t job, uint32_t cap, uint32_t* count, uint32_t* steps, float* energies,
+                      uint64_t* states) {
+  TAMC_API_BEGIN
+  return tamc_gpu_pt_gs(job_of(b, job), cap, count, steps, energies, states);
+  TAMC_API_END
+}
+int tamc_gpu_batch_samples_dims(tamc_batch* b, uint32_t job, uint32_t* M, uint32_t* S, uint32_t* Z, uint32_t* nchi) {
+  TAMC_API_BEGIN
+  return tamc_gpu_pt_samples_dims(job_of(b, job), M, S, Z, nchi);
+  TAMC_API_END
+}
+int tamc_gpu_batch_samples(tamc_batch* b, uint32_t job, float* e, int32_t* q, float* suscept, uint8_t* samples) {
+  TAMC_API_BEGIN
+  return tamc_gpu_pt_samples(job_of(b, job), e, q, suscept, samples);
+  TAMC_API_END
+}
+int tamc_gpu_batch_tile(tamc_batch* b, uint32_t job, uint32_t* cta_threads, uint32_t* slots_per_task, int32_t* csr_in_smem) {
+  TAMC_API_BEGIN
+  tamc_pt* pt = job_of(b, job);
+  if (cta_threads) *cta_threads = pt->fast->T;
+  if (slots_per_task) *slots_per_task = 4;
+  if (csr_in_smem) *csr_in_smem = pt->fast->job.csr_smem;
+  TAMC_API_END
+}
+int tamc_gpu_batch_destroy(tamc_batch* b) {
+  TAMC_API_BEGIN
+  if (!b) return TAMC_OK;
+  cudaSetDevice(b->g->device);
+  cudaStreamSynchronize(b->g->stream);
+  delete b;
+  TAMC_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,52 @@
+// fast_pt.cuh -- colour-ordered PT-ICM (TAMC_MODE_FAST): job description of the
+// fused round kernel and the glue used by the tamc_pt / tamc_batch handles.
+#pragma once
+#include "fast_common.cuh"
+#include "pt.cuh"
+
+namespace tamc {
+
+// One PT-ICM run as the fused kernel sees it.  Spins are stored slot-major:
+// W[s * nw + c * wpc + w] holds, in bit b, the spin of the replica currently at
+// temperature slot 32*w + b of chain c (1 = spin -1), sites in colour order.
+struct PtJob {
+  FastInst F;
+  uint32_t n, nt, ntp, C, wpc, nw, lo, qpc, qps;
+  int32_t icm, threaded, self_loops, csr_smem;
+  int32_t init;        // 0: load state, 1: random spins + energies, 2: load spins + energies
+  const float* betas;  // [ntp], padding slots have beta = 0
+  uint2 key;
+  uint32_t* W;         // [n][nw]
+  double* Ec;          // [C][ntp] cached energy as the reference keeps it
+  double* Er;          // [C][ntp] energy_ref of the current spins
+  uint8_t* tags;       // [C][nt]
+  uint32_t* acc;       // [C][nt]
+  uint32_t* rtrips;    // [C]
+  uint32_t* dhist;     // [C][nt][2]
+  uint32_t sweep_begin, sweep_end, num_sweeps, meas_init;
+  int64_t sample, sample_states;
+  uint32_t level, m_base, s_base;
+  MeasOut out;
+  GsLog log;
+  uint32_t* count_out; // if set: receives the log count when the job's range is done
+  uint64_t cost;       // sweeps * n * R, for longest-first ordering
+};
+
+// Shared-memory bytes the fused kernel needs for a job with T threads.
+size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem);
+// Resident CTAs per SM for the fused kernel at this size.
+int fused_blocks_per_sm(uint32_t T, size_t smem);
+// Launch over `njobs` jobs already on the device; `ctr` is a zeroed counter.
+void fused_launch(cudaStream_t st, const PtJob* d_jobs, uint32_t njobs, uint32_t* ctr, uint32_t grid,
+                  uint32_t T, size_t smem);
+
+// tamc_pt glue (single-instance handle in fast mode)
+void fast_pt_create(tamc_pt* pt, uint64_t seed);
+void fast_pt_run(tamc_pt* pt, uint32_t sweep_end);
+void fast_pt_get_state(tamc_pt* pt, int8_t* spins, float* energies);
+void fast_pt_set_state(tamc_pt* pt, const int8_t* spins);
+void fast_pt_acceptance(tamc_pt* pt, uint32_t* acc);
+void fast_pt_round_trips(tamc_pt* pt, uint8_t* tags, uint32_t* round_trips, uint32_t* dhist);
+void fast_pt_destroy(tamc_pt* pt);
+
+}  // namespace tamc

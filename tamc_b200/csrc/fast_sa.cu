@@ -1,0 +1,167 @@
+// fast_sa.cu -- colour-ordered simulated annealing (TAMC_MODE_FAST).
+//
+// One CTA owns G = 4*NQ replicas for the whole schedule; their spins live in
+// shared memory as one 32-bit word per site (bits 0..G-1), and, when it fits,
+// so does the colour-ordered CSR of the instance.  A sweep visits the colour
+// classes in order; inside a class the sites are independent, so every
+// (site, quad) task runs in parallel and the sweep is a sequential sweep in
+// colour order.  HBM is touched only to load the instance and to write the
+// final states and energies: the kernel is bound by issue (ΔE, Philox, exp),
+// not by memory.
+#include "fast_common.cuh"
+#include "fast_sa.cuh"
+
+namespace tamc {
+
+namespace {
+
+template <int NQ, bool SMEM>
+__global__ void __launch_bounds__(512) k_sa_fast(SaFastArgs a) {
+  extern __shared__ uint4 smem_u4[];
+  constexpr uint32_t G = 4 * NQ;
+  const uint32_t T = blockDim.x, tid = threadIdx.x;
+  const uint32_t n = a.F.n;
+  uint32_t* W = reinterpret_cast<uint32_t*>(smem_u4);
+  FastInst F = a.F;
+  if (SMEM) {
+    // [W: n words][rp: n+1][bias: n][pad to 8][ent: nnz uint2]
+    uint32_t* rp = W + n;
+    float* bias = reinterpret_cast<float*>(rp + n + 1);
+    uint2* ent = reinterpret_cast<uint2*>(W + ((3u * n + 1u + 1u) & ~1u));
+    for (uint32_t i = tid; i <= n; i += T) rp[i] = a.F.rp[i];
+    for (uint32_t i = tid; i < n; i += T) bias[i] = a.F.bias[i];
+    for (uint32_t i = tid; i < a.F.nnz; i += T) ent[i] = a.F.ent[i];
+    F.rp = rp;
+    F.bias = bias;
+    F.ent = ent;
+  }
+  const uint32_t r0 = blockIdx.x * G;
+  const uint2 key = a.key;
+  for (uint32_t s = tid; s < n; s += T) {
+    uint32_t w = 0;
+    if (a.init_words) {
+      w = a.init_words[(size_t)(r0 >> 5) * n + a.F.perm[s]] >> (r0 & 31u);
+      if (G < 32) w &= (1u << G) - 1u;
+    } else {
+#pragma unroll
+      for (uint32_t q = 0; q < NQ; ++q)
+        w |= init_nibble(philox4x32_10(make_uint4(s, 0xffffffffu, (r0 >> 2) + q, PTAG_INIT), key)) << (4 * q);
+    }
+    W[s] = w;
+  }
+  __syncthreads();
+  const uint32_t q = tid % NQ;
+  const uint32_t shift = 4 * q;
+  const uint32_t qid = (r0 >> 2) + q;
+  const uint32_t stride = T / NQ;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (uint32_t sw = 0; sw < a.nbeta; ++sw) {
+    const float b = a.betas[sw];
+    const float4 beta = make_float4(b, b, b, b);
+    for (uint32_t c = 0; c < F.ncolors; ++c) {
+      const uint32_t c1 = a.F.color_off[c + 1];
+      for (uint32_t s = a.F.color_off[c] + tid / NQ; s < c1; s += stride) {
+        const uint4 rnd = philox4x32_10(make_uint4(s, sw, qid, PTAG_SWEEP), key);
+        const uint32_t m = quad_update(s, shift, F, W, 1, 0, beta, rnd, acc);
+        if (m) {
+          if (NQ == 1) W[s] ^= m;
+          else atomicXor(&W[s], m << shift);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // energy_ref of every replica, f32 row terms accumulated in f64
+  double e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+  for (uint32_t s = tid / NQ; s < n; s += stride) {
+    const float4 t = energy_terms4(s, shift, F, W, 1, 0);
+    e0 += t.x;
+    e1 += t.y;
+    e2 += t.z;
+    e3 += t.w;
+  }
+#pragma unroll
+  for (uint32_t off = 16; off >= NQ; off >>= 1) {
+    e0 += __shfl_xor_sync(0xffffffffu, e0, off);
+    e1 += __shfl_xor_sync(0xffffffffu, e1, off);
+    e2 += __shfl_xor_sync(0xffffffffu, e2, off);
+    e3 += __shfl_xor_sync(0xffffffffu, e3, off);
+  }
+  __syncthreads();  // W is still read below; reuse a separate region for the reduction
+  double* red = reinterpret_cast<double*>(smem_u4) + ((SMEM ? (3u * n + 2u + 2u * a.F.nnz) : n) + 1u) / 2u + 1u;
+  const uint32_t lane = tid & 31u, warp = tid >> 5, nw = T >> 5;
+  if (lane < NQ) {
+    red[(warp * NQ + lane) * 4 + 0] = e0;
+    red[(warp * NQ + lane) * 4 + 1] = e1;
+    red[(warp * NQ + lane) * 4 + 2] = e2;
+    red[(warp * NQ + lane) * 4 + 3] = e3;
+  }
+  __syncthreads();
+  if (tid < G) {
+    double E = 0.0;
+    for (uint32_t w = 0; w < nw; ++w) E += red[(w * NQ + tid / 4) * 4 + (tid & 3u)];
+    const uint32_t r = r0 + tid;
+    if (r < a.R) a.energies_out[r] = (float)((double)a.F.offset + E);
+  }
+  // states back in original site order
+  const uint32_t keep = (a.R - r0 >= 32u) ? 0xffffffffu : ((1u << (a.R - r0)) - 1u);
+  for (uint32_t s = tid; s < n; s += T) {
+    const uint32_t v = (W[s] & (G < 32 ? ((1u << G) - 1u) : 0xffffffffu) & keep) << (r0 & 31u);
+    uint32_t* dst = a.words_out + (size_t)(r0 >> 5) * n + a.F.perm[s];
+    if (G == 32) *dst = v;
+    else atomicOr(dst, v);
+  }
+}
+
+template <int NQ, bool SMEM>
+void launch_t(cudaStream_t st, const SaFastArgs& a, uint32_t ncta, uint32_t T, size_t smem) {
+  auto k = k_sa_fast<NQ, SMEM>;
+  TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k<<<ncta, T, smem, st>>>(a);
+  TAMC_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+size_t sa_fast_smem(const FastInst& F, uint32_t nq, uint32_t T, bool smem_csr) {
+  const size_t words = smem_csr ? (3ull * F.n + 2ull + 2ull * F.nnz) : (size_t)F.n;
+  return ((words + 1) / 2 + 1) * 8 + (size_t)(T / 32) * nq * 4 * 8 + 16;
+}
+
+SaTile sa_fast_choose(const tamc_gpu* g, const FastInst& F, uint32_t R) {
+  SaTile t;
+  t.T = 512;
+  t.smem_csr = sa_fast_smem(F, 8, t.T, true) <= g->smem_optin;
+  // smallest replica group that still gives every SM a CTA
+  t.nq = 8;
+  for (uint32_t nq : {1u, 2u, 4u, 8u}) {
+    const uint32_t ncta = (R + 4 * nq - 1) / (4 * nq);
+    if (ncta <= (uint32_t)g->num_sms) { t.nq = nq; break; }
+  }
+  if (const char* e = getenv("TAMC_SA_NQ")) {
+    const int v = atoi(e);
+    if (v == 1 || v == 2 || v == 4 || v == 8) t.nq = (uint32_t)v;
+  }
+  t.smem = sa_fast_smem(F, t.nq, t.T, t.smem_csr);
+  if (t.smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the fast SA kernel");
+  return t;
+}
+
+void sa_fast_launch(cudaStream_t st, const SaFastArgs& a, const SaTile& t) {
+  const uint32_t G = 4 * t.nq;
+  const uint32_t ncta = (a.R + G - 1) / G;
+  if (!ncta) return;
+  switch (t.nq * 2 + (t.smem_csr ? 1 : 0)) {
+    case 2: launch_t<1, false>(st, a, ncta, t.T, t.smem); break;
+    case 3: launch_t<1, true>(st, a, ncta, t.T, t.smem); break;
+    case 4: launch_t<2, false>(st, a, ncta, t.T, t.smem); break;
+    case 5: launch_t<2, true>(st, a, ncta, t.T, t.smem); break;
+    case 8: launch_t<4, false>(st, a, ncta, t.T, t.smem); break;
+    case 9: launch_t<4, true>(st, a, ncta, t.T, t.smem); break;
+    case 16: launch_t<8, false>(st, a, ncta, t.T, t.smem); break;
+    case 17: launch_t<8, true>(st, a, ncta, t.T, t.smem); break;
+    default: fail(TAMC_E_INVAL, "bad SA tile");
+  }
+}
+
+}  // namespace tamc

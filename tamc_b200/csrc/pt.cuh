@@ -1,0 +1,109 @@
+// pt.cuh -- the PT-ICM run handle shared by the reference-order and fast paths.
+#pragma once
+#include <chrono>
+#include <memory>
+
+#include "fast_common.cuh"
+#include "ref_kernels.cuh"
+
+namespace tamc {
+
+template <class T>
+struct DBuf {  // owning device buffer
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  explicit DBuf(size_t count) { alloc(count); }
+  void alloc(size_t count) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = count;
+    TAMC_CUDA(cudaMalloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T)));
+  }
+  void zero(cudaStream_t st) { TAMC_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), st)); }
+  ~DBuf() {
+    if (p) cudaFree(p);
+  }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+};
+
+// Resolved run configuration (PtIcmParams + PtIcmRunner::new, src/pt.rs:307-351).
+struct PtCfg {
+  uint32_t num_sweeps = 0;
+  double warmup = 0;
+  std::vector<float> betas;
+  uint32_t nt = 0, C = 0, lo = 0;
+  bool icm = false;
+  uint32_t threads = 1;
+  int64_t sample = -1, sample_states = -1;
+  uint32_t level = 0;
+  uint32_t meas_init = 0;
+  uint32_t M = 0, S = 0, Z = 0;  // measurements, state snapshots, sample slots
+  bool is_meas(uint32_t i) const {
+    return sample >= 0 && i >= meas_init && ((i - meas_init) % (uint32_t)sample == 0 || i == num_sweeps - 1);
+  }
+  bool is_snap(uint32_t i) const {
+    return sample_states >= 0 && i >= meas_init &&
+           ((i - meas_init) % (uint32_t)sample_states == 0 || i == num_sweeps - 1);
+  }
+};
+PtCfg make_cfg(const tamc_pt_params* p);
+
+// Device output buffers and the host-side ground-state trajectory.
+struct PtOutputs {
+  uint32_t n = 0, nchi = 0;
+  DBuf<float> e;
+  DBuf<int32_t> q;
+  DBuf<float> sus;
+  DBuf<uint8_t> samp;
+  DBuf<uint32_t> gs_count;
+  DBuf<int> gs_have;
+  DBuf<float> gs_min;
+  DBuf<uint32_t> gs_steps;
+  DBuf<float> gs_E;
+  DBuf<uint64_t> gs_words;
+  uint32_t cap = 0;
+  uint32_t pending = 0;  // tracked sweeps since the last drain
+  std::vector<uint32_t> h_steps;
+  std::vector<float> h_E;
+  std::vector<uint64_t> h_words;  // concatenated
+  void init(const PtCfg& c, uint32_t n_, uint32_t nchi_, cudaStream_t st);
+  MeasOut meas(const PtCfg& c) const;
+  GsLog log() const;
+  void drain(cudaStream_t st);  // synchronous
+};
+
+}  // namespace tamc
+
+struct tamc_pt {
+  tamc_inst* inst = nullptr;
+  tamc_gpu* g = nullptr;
+  int mode = 0;
+  tamc::PtCfg cfg;
+  uint32_t next_sweep = 0;
+  uint32_t m_next = 0, s_next = 0;  // next measurement / snapshot index
+  double timing_us = 0;
+  bool running = false;
+  std::chrono::steady_clock::time_point t0;
+  tamc::PtOutputs out;
+  // reference-order state
+  tamc::DBuf<int8_t> spins;
+  tamc::DBuf<float> energy;
+  tamc::DBuf<uint32_t> perm;
+  tamc::DBuf<uint8_t> tags;
+  tamc::DBuf<uint32_t> acc;
+  tamc::DBuf<uint32_t> rtrips;
+  tamc::DBuf<uint32_t> dhist;
+  tamc::DBuf<float> e_stale;
+  tamc::DBuf<float> d_betas;
+  tamc::DBuf<float> d_dbeta;
+  tamc::DBuf<uint32_t> visited;
+  tamc::DBuf<uint32_t> queue;
+  tamc::DBuf<float> rows;
+  tamc::DBuf<tamc::Xo> rng;
+  tamc::DBuf<int> err;
+  // fast-mode state lives behind an opaque pointer (fast_pt.cu)
+  struct FastState;
+  FastState* fast = nullptr;
+};
