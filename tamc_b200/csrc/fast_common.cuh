@@ -65,9 +65,19 @@ __device__ __forceinline__ bool accept1(float dE, float beta, uint32_t r) {
   return (float)(r >> 8) * (1.0f / 16777216.0f) < p;
 }
 
+// Energies are accumulated in 64-bit fixed point with 2^-32 resolution:
+// integer addition is associative, so sums do not depend on how sites are
+// spread over threads (CTA size, batching) and results are bit-reproducible.
+#define TAMC_FX_SCALE 4294967296.0f
+#define TAMC_FX_INV 2.3283064365386963e-10
+__device__ __forceinline__ long long to_fx(float x) { return __float2ll_rn(x * TAMC_FX_SCALE); }
+struct Fx4 {
+  long long x, y, z, w;
+};
+
 // One quad update.  Returns the 4-bit flip mask; adds accepted ΔE to acc.
 __device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
-                                                uint32_t ws, uint32_t wo, float4 beta, uint4 rnd, float4& acc) {
+                                                uint32_t ws, uint32_t wo, float4 beta, uint4 rnd, Fx4& acc) {
   const float4 f = local_field4(s, shift, F.rp, F.ent, F.bias, W, ws, wo);
   const uint32_t own = W[s * ws + wo] >> shift;
   const float4 d = delta4(f, own);
@@ -75,10 +85,10 @@ __device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, cons
   const bool a1 = accept1(d.y, beta.y, rnd.y);
   const bool a2 = accept1(d.z, beta.z, rnd.z);
   const bool a3 = accept1(d.w, beta.w, rnd.w);
-  acc.x += a0 ? d.x : 0.0f;
-  acc.y += a1 ? d.y : 0.0f;
-  acc.z += a2 ? d.z : 0.0f;
-  acc.w += a3 ? d.w : 0.0f;
+  acc.x += to_fx(a0 ? d.x : 0.0f);
+  acc.y += to_fx(a1 ? d.y : 0.0f);
+  acc.z += to_fx(a2 ? d.z : 0.0f);
+  acc.w += to_fx(a3 ? d.w : 0.0f);
   return (uint32_t)a0 | ((uint32_t)a1 << 1) | ((uint32_t)a2 << 2) | ((uint32_t)a3 << 3);
 }
 

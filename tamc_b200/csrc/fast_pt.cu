@@ -112,17 +112,17 @@ __device__ void full_energies(const PtJob& J, const FastInst& F, Smem& S, uint32
   const uint32_t k = tid % J.qps;
   const uint32_t ch = k / J.qpc, q = k % J.qpc;
   const uint32_t wo = ch * J.wpc + (q >> 3), shift = 4 * (q & 7u);
-  double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
   if (tid < Teff) {
     for (uint32_t s = tid / J.qps; s < J.n; s += Teff / J.qps) {
       const float4 e = energy_terms4(s, shift, F, S.W, J.nw, wo);
-      a0 += e.x;
-      a1 += e.y;
-      a2 += e.z;
-      a3 += e.w;
+      a0 += to_fx(e.x);
+      a1 += to_fx(e.y);
+      a2 += to_fx(e.z);
+      a3 += to_fx(e.w);
     }
   }
-  double* redd = reinterpret_cast<double*>(S.red);  // red and redq are contiguous: 2*T float4 = T double4
+  long long* redd = reinterpret_cast<long long*>(S.red);  // red and redq are contiguous: 2*T*16 bytes
   __syncthreads();
   if (tid < Teff) {
     redd[tid * 4 + 0] = a0;
@@ -134,9 +134,9 @@ __device__ void full_energies(const PtJob& J, const FastInst& F, Smem& S, uint32
   for (uint32_t x = tid; x < J.C * J.ntp; x += blockDim.x) {
     const uint32_t c = x / J.ntp, t = x % J.ntp;
     const uint32_t kk = c * J.qpc + t / 4;
-    double sum = 0;
+    long long sum = 0;
     for (uint32_t th = kk; th < Teff; th += J.qps) sum += redd[th * 4 + (t & 3u)];
-    S.Ec[x] = (double)J.F.offset + sum;
+    S.Ec[x] = (double)J.F.offset + (double)sum * TAMC_FX_INV;
     S.Er[x] = S.Ec[x];
   }
   __syncthreads();
@@ -371,8 +371,8 @@ __device__ void sweep_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t
   const uint32_t qid = ch * 16u + q;
   const float4 beta = S.beta4[k];
   const uint32_t stride = Teff / J.qps;
-  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  float4 qacc = make_float4(0.f, 0.f, 0.f, 0.f);
+  Fx4 acc{0, 0, 0, 0};
+  Fx4 qacc{0, 0, 0, 0};
   for (uint32_t c = 0; c < F.ncolors; ++c) {
     if (tid < Teff) {
       const uint32_t c1 = J.F.color_off[c + 1];
@@ -382,35 +382,51 @@ __device__ void sweep_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t
         if (m) {
           atomicXor(&S.W[s * J.nw + wo], m << shift);
           if (SELF) {
-            const float k2 = 2.0f * J.F.kd[s];
-            qacc.x += (m & 1u) ? k2 : 0.0f;
-            qacc.y += (m & 2u) ? k2 : 0.0f;
-            qacc.z += (m & 4u) ? k2 : 0.0f;
-            qacc.w += (m & 8u) ? k2 : 0.0f;
+            const long long k2 = to_fx(2.0f * J.F.kd[s]);
+            qacc.x += (m & 1u) ? k2 : 0;
+            qacc.y += (m & 2u) ? k2 : 0;
+            qacc.z += (m & 4u) ? k2 : 0;
+            qacc.w += (m & 8u) ? k2 : 0;
           }
         }
       }
     }
     __syncthreads();
   }
-  S.red[tid] = acc;
-  if (SELF) S.redq[tid] = qacc;
+  Fx4* red = reinterpret_cast<Fx4*>(S.red);   // T Fx4 = red + redq (2 * T * 16 bytes)
+  red[tid] = acc;
   __syncthreads();
-  for (uint32_t x = tid; x < J.C * J.ntp; x += blockDim.x) {
+  long long sums[4] = {0, 0, 0, 0};
+  for (uint32_t x = tid, r = 0; x < J.C * J.ntp && r < 4; x += blockDim.x, ++r) {
     const uint32_t c = x / J.ntp, t = x % J.ntp;
     const uint32_t kk = c * J.qpc + t / 4;
-    float sum = 0.0f, qs = 0.0f;
+    long long sum = 0;
     for (uint32_t th = kk; th < Teff; th += J.qps) {
-      const float4 v = S.red[th];
+      const Fx4 v = red[th];
       sum += (t & 3u) == 0 ? v.x : (t & 3u) == 1 ? v.y : (t & 3u) == 2 ? v.z : v.w;
-      if (SELF) {
-        const float4 w = S.redq[th];
-        qs += (t & 3u) == 0 ? w.x : (t & 3u) == 1 ? w.y : (t & 3u) == 2 ? w.z : w.w;
-      }
     }
-    // IsingSampler::sweep: energy += Σ accepted ΔE (src/ising.rs:226-232)
-    S.Ec[x] += (double)sum;
-    S.Er[x] += (double)sum + (double)qs;
+    sums[r] = sum;
+  }
+  long long qsums[4] = {0, 0, 0, 0};
+  if (SELF) {
+    __syncthreads();
+    red[tid] = qacc;
+    __syncthreads();
+    for (uint32_t x = tid, r = 0; x < J.C * J.ntp && r < 4; x += blockDim.x, ++r) {
+      const uint32_t c = x / J.ntp, t = x % J.ntp;
+      const uint32_t kk = c * J.qpc + t / 4;
+      long long q = 0;
+      for (uint32_t th = kk; th < Teff; th += J.qps) {
+        const Fx4 v = red[th];
+        q += (t & 3u) == 0 ? v.x : (t & 3u) == 1 ? v.y : (t & 3u) == 2 ? v.z : v.w;
+      }
+      qsums[r] = q;
+    }
+  }
+  // IsingSampler::sweep: energy += Σ accepted ΔE (src/ising.rs:226-232)
+  for (uint32_t x = tid, r = 0; x < J.C * J.ntp && r < 4; x += blockDim.x, ++r) {
+    S.Ec[x] += (double)sums[r] * TAMC_FX_INV;
+    S.Er[x] += (double)(sums[r] + qsums[r]) * TAMC_FX_INV;
   }
   __syncthreads();
 }

