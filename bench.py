@@ -192,7 +192,10 @@ def run_gpu(args):
     energies = torch.empty(N_REPLICAS, dtype=torch.float32, device=dev)
     words = torch.empty(((N_REPLICAS + 31) // 32) * N_SPINS, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream: its handle is never 0, so the library launches on it
+    # and the CUDA events below time exactly those launches
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     seed0 = 1000 * (rank + 1)
 
     def step(k):
@@ -272,6 +275,187 @@ def run_gpu(args):
     return 0
 
 
+# ------------------------------------------------------- other workloads ----
+# The remaining benchmark configurations, run with --workload; each prints one
+# JSON line.  They are measured separately from the headline line above.
+def _lattice_params(tb, nt, sweeps, sample=None, states=None, level=0, threads=8):
+    b = tb.geometric_betas(0.2, 5.0, nt)
+    lo = int(np.argmax(b >= np.float32(1.0))) if np.any(b >= np.float32(1.0)) else nt - 1
+    return tb.PtParams(sweeps, b, lo, 0.5, True, 2, threads, sample, states, level)
+
+
+def _time_run(tb, dinst, p, seed):
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = tb.PtRun(dinst, p, seed).run().sync()
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0, r
+
+
+def workload_pt_c1(args, tb, gi, gpu):
+    """2-D EA +-J, L=16, nt=32, 2 chains, ICM, 2000 sweeps, sample 32 / states 32 / limiting 2."""
+    text = gi.lattice(16, 2, "pm", 0)
+    d = gpu.upload(tb.HostInstance.parse(text))
+    p = _lattice_params(tb, 32, 2000, 32, 32, 2, threads=1)
+    flips = 256 * 32 * 2 * 2000
+    _time_run(tb, d, p, 1)
+    t_fast, r = _time_run(tb, d, p, 2)
+    t0 = time.perf_counter()
+    rr = tb.PtRun(d, p, 3, tb.MODE_REF).run().sync()
+    t_ref = time.perf_counter() - t0
+    out = {"workload": "pt_c1", "flips": flips, "fast_flips_per_s": flips / t_fast, "fast_s": t_fast,
+           "ref_mode_flips_per_s": flips / t_ref, "ref_mode_s": t_ref,
+           "best_energy_fast": float(r.gs()[1][-1]), "best_energy_ref_mode": float(rr.gs()[1][-1])}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        inst = po.Instance.from_text(text)
+        t0 = time.perf_counter()
+        orc = po.PtRun(inst, p.betas, 2000, 0.5, p.lo_beta_idx, True, 2, 1, sample=32, sample_states=32,
+                       sample_limiting=2, seed=3)
+        orc.run()
+        t_cpu = time.perf_counter() - t0
+        out.update(cpu_flips_per_s=flips / t_cpu, cpu_s=t_cpu, cpu_kind="oracle, threads: 1 (serial reference loop)",
+                   cpu_best_energy=float(orc.gs()[-1][1]))
+    return out
+
+
+def workload_batch_c3(args, tb, gi, gpu):
+    """256 uneven 2-D +-J instances, L in {8..32}, nt in {16,24,32}, 5000 sweeps: batched vs plain."""
+    rng = np.random.default_rng(0)
+    jobs = []
+    for k in range(256):
+        L = int(rng.choice([8, 12, 16, 24, 32]))
+        nt = int(rng.choice([16, 24, 32]))
+        jobs.append((L, nt))
+    sweeps = args.c3_sweeps
+    dinsts = {}
+    batch = tb.Batch(gpu)
+    flips = 0
+    for k, (L, nt) in enumerate(jobs):
+        key = (L, k)
+        d = gpu.upload(tb.HostInstance.parse(gi.lattice(L, 2, "pm", 1000 + k)))
+        dinsts[key] = d
+        batch.add(d, _lattice_params(tb, nt, sweeps), 7 + k)
+        flips += L * L * nt * 2 * sweeps
+    import torch
+    torch.cuda.synchronize()
+    l0 = gpu.launches
+    t0 = time.perf_counter()
+    batch.run()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    l_batch = gpu.launches - l0
+    # plain form (one instance at a time, one launch per sweep phase) on a subset
+    os.environ["TAMC_PT_FORM"] = "plain"
+    sub = list(range(0, 256, 16))
+    f_sub, t_sub = 0, 0.0
+    for k in sub:
+        L, nt = jobs[k]
+        d = dinsts[(L, k)]
+        p = _lattice_params(tb, nt, sweeps)
+        t, _ = _time_run(tb, d, p, 7 + k)
+        t_sub += t
+        f_sub += L * L * nt * 2 * sweeps
+    del os.environ["TAMC_PT_FORM"]
+    plain_rate = f_sub / t_sub
+    return {"workload": "batch_c3", "instances": 256, "sweeps": sweeps, "flips": flips,
+            "batched_flips_per_s": flips / t_batch, "batched_s": t_batch, "batched_launches": int(l_batch),
+            "plain_flips_per_s": plain_rate, "plain_sample": f"{len(sub)} of 256 instances",
+            "batched_over_plain": (flips / t_batch) / plain_rate}
+
+
+def workload_pt_c4(args, tb, gi, gpu):
+    """3-D Gaussian L=16 (N=4096), nt=64, 2 chains, ICM, 20000 sweeps, sampling every 32, suscepts."""
+    L = 16
+    text = gi.lattice(L, 3, "gauss", 0)
+    h = tb.HostInstance.parse(text)
+    w = [gi.fourier_weights(L, 3, 0), gi.fourier_weights(L, 3, 1)]
+    for row in w:
+        h.add_suscept(row)
+    d = gpu.upload(h)
+    sweeps = args.c4_sweeps
+    p = _lattice_params(tb, 64, sweeps, 32, 32, 0, threads=64)
+    flips = 4096 * 64 * 2 * sweeps
+    _time_run(tb, d, _lattice_params(tb, 64, 64, 32, 32, 0, threads=64), 1)  # autotune + warm-up
+    t_gpu, r = _time_run(tb, d, p, 2)
+    out = {"workload": "pt_c4", "sweeps": sweeps, "flips": flips, "gpu_flips_per_s": flips / t_gpu, "gpu_s": t_gpu,
+           "gpu_best_energy": float(r.gs()[1][-1])}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        inst = po.Instance.from_text(text)
+        for row in w:
+            inst.add_suscept(row)
+        k = args.c4_cpu_sweeps
+        cores = os.cpu_count() or 1
+        orc = po.PtRun(inst, p.betas, k, 0.0, p.lo_beta_idx, True, 2, 64, sample=32, sample_states=32,
+                       sample_limiting=0, seed=3)
+        t0 = time.perf_counter()
+        orc.run(nthreads=cores)
+        t_cpu = time.perf_counter() - t0
+        cpu_rate = 4096 * 64 * 2 * k / t_cpu
+        out.update(cpu_flips_per_s=cpu_rate, cpu_sample=f"oracle run_parallel (threads: 64), first {k} sweeps "
+                   f"measured every sweep, {cores} OpenMP threads", cpu_cores=cores,
+                   gpu_over_cpu=(flips / t_gpu) / cpu_rate)
+    return out
+
+
+def workload_serve_c5(args, tb, gi, gpu):
+    """Poisson stream of QUBO requests, N log-uniform in [64, 8192], PT-ICM 16-32 temps, 1000 sweeps."""
+    rng = np.random.default_rng(5)
+    nreq = args.c5_requests
+    reqs = []
+    for k in range(nreq):
+        n = int(round(math.exp(rng.uniform(math.log(64), math.log(8192)))))
+        nt = int(rng.integers(16, 33))
+        reqs.append((n, nt))
+    texts = [gi.qubo_er(n, 6.0, 100 + k) for k, (n, _) in enumerate(reqs)]
+    hosts = [tb.HostInstance.parse(t, qubo=True) for t in texts]
+    rate = args.c5_rate
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    srv = tb.Server(gpu, hbm_budget_bytes=64 << 30, max_active=512, chunk_sweeps=125)
+    ids = {}
+    t0 = time.perf_counter()
+    nxt = 0
+    while True:
+        now = time.perf_counter() - t0
+        while nxt < nreq and arrivals[nxt] <= now:
+            n, nt = reqs[nxt]
+            b = tb.geometric_betas(0.2, 5.0, nt)
+            lo = int(np.argmax(b >= np.float32(1.0)))
+            ids[nxt] = srv.submit(hosts[nxt], tb.PtParams(1000, b, lo, 0.5, True, 2, 8), 900 + nxt)
+            nxt += 1
+        a, q = srv.step()
+        if nxt >= nreq and a == 0 and q == 0:
+            break
+        if a == 0 and q == 0 and nxt < nreq:
+            time.sleep(max(0.0, min(0.01, arrivals[nxt] - (time.perf_counter() - t0))))
+    wall = time.perf_counter() - t0
+    lat = np.array([srv.result(ids[k])[3] for k in range(nreq)])
+    flips = sum(n * nt * 2 * 1000 for n, nt in reqs)
+    return {"workload": "serve_c5", "requests": nreq, "offered_rate_per_s": rate, "wall_s": wall,
+            "flips": flips, "aggregate_flips_per_s": flips / wall, "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean())}
+
+
+def run_workload(args):
+    import torch
+    import tamc_b200 as tb
+    from tamc_b200 import instances as gi
+    torch.cuda.set_device(0)
+    gpu = tb.Gpu(0)
+    fn = {"pt_c1": workload_pt_c1, "batch_c3": workload_batch_c3, "pt_c4": workload_pt_c4,
+          "serve_c5": workload_serve_c5}[args.workload]
+    with ClockSampler(0) as clk:
+        out = fn(args, tb, gi, gpu)
+    out["metric"] = "spin-flip attempts/s"
+    out["clocks"] = clk.summary()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -279,11 +463,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--workload", default="sa_c2", choices=["sa_c2", "pt_c1", "batch_c3", "pt_c4", "serve_c5"])
+    ap.add_argument("--c3-sweeps", type=int, default=5000)
+    ap.add_argument("--c4-sweeps", type=int, default=20000)
+    ap.add_argument("--c4-cpu-sweeps", type=int, default=200)
+    ap.add_argument("--c5-requests", type=int, default=1000)
+    ap.add_argument("--c5-rate", type=float, default=100.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "sa_c2":
+        return run_workload(args)
     return run_gpu(args)
 
 

@@ -61,6 +61,29 @@ static T* dmalloc_copy(const T* h, size_t count) {
 
 using namespace tamc;
 
+void tamc_gpu_retain(tamc_gpu* g) { g->refs.fetch_add(1); }
+void tamc_gpu_release(tamc_gpu* g) {
+  if (g->refs.fetch_sub(1) != 1) return;
+  cudaSetDevice(g->device);
+  cudaStreamSynchronize(g->stream);
+  cudaFree(g->d_exp);
+  cudaStreamDestroy(g->stream);
+  delete g;
+}
+void tamc_inst_retain(tamc_inst* d) { d->refs.fetch_add(1); }
+void tamc_inst_release(tamc_inst* d) {
+  if (d->refs.fetch_sub(1) != 1) return;
+  tamc_gpu* g = d->g;
+  cudaSetDevice(g->device);
+  void* ptrs[] = {d->d_rp, d->d_col, d->d_J, d->d_bias, d->d_grp, d->d_gcol, d->d_sus, d->d_color_off,
+                  d->d_perm, d->d_iperm, d->d_frp, d->d_fent, d->d_fbias, d->d_fkd, d->d_fsus};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  d->sa_scratch.release();
+  delete d;
+  tamc_gpu_release(g);
+}
+
 extern "C" {
 
 int tamc_gpu_open(int device, tamc_gpu** out) {
@@ -102,11 +125,7 @@ int tamc_gpu_open(int device, tamc_gpu** out) {
 int tamc_gpu_close(tamc_gpu* g) {
   TAMC_API_BEGIN
   if (!g) return TAMC_OK;
-  cudaSetDevice(g->device);
-  cudaStreamSynchronize(g->stream);
-  cudaFree(g->d_exp);
-  cudaStreamDestroy(g->stream);
-  delete g;
+  tamc_gpu_release(g);
   TAMC_API_END
 }
 
@@ -134,6 +153,7 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
   const HostInstance& h = hi->h;
   auto* d = new tamc_inst();
   d->g = g;
+  tamc_gpu_retain(g);
   d->host = h;
   d->n = h.n;
   d->nnz = h.col.size();
@@ -210,12 +230,7 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
 int tamc_gpu_instance_destroy(tamc_inst* d) {
   TAMC_API_BEGIN
   if (!d) return TAMC_OK;
-  cudaSetDevice(d->g->device);
-  void* ptrs[] = {d->d_rp, d->d_col, d->d_J, d->d_bias, d->d_grp, d->d_gcol, d->d_sus, d->d_color_off,
-                  d->d_perm, d->d_iperm, d->d_frp, d->d_fent, d->d_fbias, d->d_fkd, d->d_fsus};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
-  delete d;
+  tamc_inst_release(d);
   TAMC_API_END
 }
 

@@ -101,7 +101,43 @@ struct tamc_gpu {
   uint32_t* d_exp = nullptr;  // exception table blob
   tamc::ExpTable exp{};
   std::atomic<uint64_t> launches{0};
+  // Handles created from this context (instances, batches, servers) hold a
+  // reference; tamc_gpu_close only drops the caller's reference, so a
+  // context is released after its last child whatever the destruction order.
+  std::atomic<int> refs{1};
   void count(uint64_t k = 1) { launches.fetch_add(k, std::memory_order_relaxed); }
+};
+void tamc_gpu_retain(tamc_gpu* g);
+void tamc_gpu_release(tamc_gpu* g);
+
+// Reusable device buffers of the host-buffer SA entry point.
+struct SaScratch {
+  uint32_t* words = nullptr;
+  float* energies = nullptr;
+  uint8_t* packed = nullptr;
+  size_t cap_words = 0, cap_e = 0, cap_packed = 0;
+  void ensure(size_t nwords, size_t ne, size_t npacked) {
+    auto grow = [](auto*& p, size_t& cap, size_t want, size_t elt) {
+      if (want <= cap) return;
+      if (p) cudaFree(p);
+      p = nullptr;
+      cap = 0;
+      if (cudaMalloc((void**)&p, want * elt) != cudaSuccess) tamc::fail(TAMC_E_NOMEM, "device allocation failed");
+      cap = want;
+    };
+    grow(words, cap_words, nwords, 4);
+    grow(energies, cap_e, ne, 4);
+    grow(packed, cap_packed, npacked, 1);
+  }
+  void release() {
+    if (words) cudaFree(words);
+    if (energies) cudaFree(energies);
+    if (packed) cudaFree(packed);
+    words = nullptr;
+    energies = nullptr;
+    packed = nullptr;
+    cap_words = cap_e = cap_packed = 0;
+  }
 };
 
 // Device-resident instance.  Two site orders are kept:
@@ -112,6 +148,7 @@ struct tamc_gpu {
 //    per-row order so ΔE is summed in the same order as the reference.
 struct tamc_inst {
   tamc_gpu* g = nullptr;
+  std::atomic<int> refs{1};  // runs created on the instance hold a reference
   uint32_t n = 0;
   uint64_t nnz = 0;
   float offset = 0.0f;
@@ -141,4 +178,7 @@ struct tamc_inst {
   // host copies used by drivers
   tamc::HostInstance host;
   std::vector<uint32_t> h_perm;
+  SaScratch sa_scratch;
 };
+void tamc_inst_retain(tamc_inst* d);
+void tamc_inst_release(tamc_inst* d);

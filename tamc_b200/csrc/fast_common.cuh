@@ -58,11 +58,18 @@ __device__ __forceinline__ float4 delta4(float4 f, uint32_t own) {
   return d;
 }
 
-// Metropolis rule: accept iff u < exp(-beta * max(ΔE, 0)) with u a 24-bit
-// uniform; ΔE <= 0 always accepts (p = 1), as the reference's rule does.
-__device__ __forceinline__ bool accept1(float dE, float beta, uint32_t r) {
-  const float p = __expf(-beta * fmaxf(dE, 0.0f));
-  return (float)(r >> 8) * (1.0f / 16777216.0f) < p;
+// Metropolis rule: accept iff u < 2^(-beta*log2(e) * max(ΔE, 0)); ΔE <= 0
+// always accepts (p = 1), as the reference's rule does.  `bl2` is beta*log2(e);
+// u is a 23-bit uniform built by placing the random mantissa under the
+// exponent of 1.0 (u + 1 in [1, 2)), compared with p + 1.
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ bool accept1(float dE, float bl2, uint32_t r) {
+  const float p1 = ex2_approx(-bl2 * fmaxf(dE, 0.0f)) + 1.0f;
+  return __uint_as_float(0x3f800000u | (r >> 9)) < p1;
 }
 
 // Energies are accumulated in 64-bit fixed point with 2^-32 resolution:
@@ -75,20 +82,24 @@ struct Fx4 {
   long long x, y, z, w;
 };
 
-// One quad update.  Returns the 4-bit flip mask; adds accepted ΔE to acc.
+// One quad update with inverse temperatures pre-scaled by log2(e).  Returns
+// the 4-bit flip mask; with ACC, adds accepted ΔE to acc in fixed point.
+template <bool ACC>
 __device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
-                                                uint32_t ws, uint32_t wo, float4 beta, uint4 rnd, Fx4& acc) {
+                                                uint32_t ws, uint32_t wo, float4 bl2, uint4 rnd, Fx4& acc) {
   const float4 f = local_field4(s, shift, F.rp, F.ent, F.bias, W, ws, wo);
   const uint32_t own = W[s * ws + wo] >> shift;
   const float4 d = delta4(f, own);
-  const bool a0 = accept1(d.x, beta.x, rnd.x);
-  const bool a1 = accept1(d.y, beta.y, rnd.y);
-  const bool a2 = accept1(d.z, beta.z, rnd.z);
-  const bool a3 = accept1(d.w, beta.w, rnd.w);
-  acc.x += to_fx(a0 ? d.x : 0.0f);
-  acc.y += to_fx(a1 ? d.y : 0.0f);
-  acc.z += to_fx(a2 ? d.z : 0.0f);
-  acc.w += to_fx(a3 ? d.w : 0.0f);
+  const bool a0 = accept1(d.x, bl2.x, rnd.x);
+  const bool a1 = accept1(d.y, bl2.y, rnd.y);
+  const bool a2 = accept1(d.z, bl2.z, rnd.z);
+  const bool a3 = accept1(d.w, bl2.w, rnd.w);
+  if (ACC) {
+    acc.x += to_fx(a0 ? d.x : 0.0f);
+    acc.y += to_fx(a1 ? d.y : 0.0f);
+    acc.z += to_fx(a2 ? d.z : 0.0f);
+    acc.w += to_fx(a3 ? d.w : 0.0f);
+  }
   return (uint32_t)a0 | ((uint32_t)a1 << 1) | ((uint32_t)a2 << 2) | ((uint32_t)a3 << 3);
 }
 

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -21,7 +22,19 @@ struct tamc_pt::FastState {
   tamc::DBuf<uint32_t> ctr;
   uint32_t T = 512;
   size_t smem = 0;
+  // plain form (one instance over the whole GPU)
+  bool plain = false;
+  tamc::DBuf<tamc::PlainCtl> ctl;
+  tamc::DBuf<long long> eacc;  // fixed-point sweep sums (2 x C x ntp)
+  size_t head_smem = 0;
+  uint32_t grid_cap = 0;
+  std::map<uint32_t, cudaGraphExec_t> graphs;  // captured chunks of K rounds
+  ~FastState() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+  }
 };
+
+bool tamc_pt::fast_plain() const { return fast && fast->plain; }
 
 namespace tamc {
 
@@ -94,7 +107,12 @@ static float time_tile(tamc_gpu* g, const PtJob& proto, TileChoice t, uint32_t r
   return ms;
 }
 
+// Set while a server creates runs: every request has its own shape, so the
+// timing autotuner would run per request; the heuristic tile is used instead.
+thread_local bool g_no_autotune = false;
+
 static TileChoice tune_tile(tamc_gpu* g, const PtJob& j) {
+  if (g_no_autotune) return heuristic_tile(g, j);
   const auto key = std::make_tuple(g->device, j.n, j.F.nnz, j.nt, j.C, (int)j.self_loops);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -209,9 +227,136 @@ static void launch_one(tamc_pt* pt, uint32_t begin, uint32_t end, int init) {
   TAMC_CUDA(cudaStreamSynchronize(st));
 }
 
+// ---- plain form: one launch per sweep phase over the whole GPU
+static void plain_enqueue_rounds(tamc_pt* pt, uint32_t K) {
+  auto* F = pt->fast;
+  const PtJob& j = F->job;
+  cudaStream_t st = pt->g->stream;
+  const auto& off = pt->inst->color_off;
+  for (uint32_t r = 0; r < K; ++r) {
+    plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 0, F->head_smem);
+    for (uint32_t c = 0; c + 1 < off.size(); ++c)
+      plain_launch_sweep(st, j, F->d_job.p, F->ctl.p, c, (off[c + 1] - off[c]) * j.qps, F->eacc.p, F->grid_cap);
+  }
+  plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem);  // close the last round
+}
+
+static void plain_run_chunk(tamc_pt* pt, uint32_t K) {
+  auto* F = pt->fast;
+  cudaStream_t st = pt->g->stream;
+  auto it = F->graphs.find(K);
+  if (it == F->graphs.end()) {
+    cudaGraph_t graph;
+    TAMC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    plain_enqueue_rounds(pt, K);
+    TAMC_CUDA(cudaStreamEndCapture(st, &graph));
+    cudaGraphExec_t exec;
+    TAMC_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    it = F->graphs.emplace(K, exec).first;
+  }
+  TAMC_CUDA(cudaGraphLaunch(it->second, st));
+  pt->g->count((uint64_t)K * (1 + pt->inst->ncolors) + 1);
+}
+
+static void plain_setup(tamc_pt* pt) {
+  auto* F = pt->fast;
+  PtJob& j = F->job;
+  cudaStream_t st = pt->g->stream;
+  F->plain = true;
+  F->head_smem = plain_head_bytes(j);
+  if (F->head_smem > pt->g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the plain PT head kernel");
+  F->grid_cap = (uint32_t)pt->g->num_sms * 8;
+  F->ctl.alloc(1);
+  F->ctl.zero(st);
+  F->eacc.alloc(2 * (size_t)j.C * j.ntp);
+  F->eacc.zero(st);
+  j.init = 0;
+  j.count_out = nullptr;
+  TAMC_CUDA(cudaMemcpyAsync(F->d_job.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
+}
+
+static void plain_init_energies(tamc_pt* pt, bool random) {
+  auto* F = pt->fast;
+  cudaStream_t st = pt->g->stream;
+  F->eacc.zero(st);
+  plain_launch_init(st, F->d_job.p, F->eacc.p, random ? 1 : 0, (uint32_t)pt->g->num_sms * 4);
+  plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 2, F->head_smem);
+  pt->g->count(random ? 3 : 2);
+  TAMC_CUDA(cudaStreamSynchronize(st));
+}
+
+// Which form runs a single instance: the fused kernel (one CTA, state in
+// shared memory) or the plain form (all SMs, state in L2/HBM).  Both give the
+// same results; the autotuner times a few rounds of each on this shape.
+static std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t>, bool> g_form;
+
+static bool choose_plain(tamc_pt* pt) {
+  const char* f = getenv("TAMC_PT_FORM");
+  if (f && !strcmp(f, "plain")) return true;
+  if (f && !strcmp(f, "fused")) return false;
+  if (g_no_autotune) return fused_smem_bytes(pt->fast->job, 512, false) > pt->g->smem_optin;
+  const PtJob& j = pt->fast->job;
+  const bool fused_fits = fused_smem_bytes(j, 128, false) <= pt->g->smem_optin;
+  const bool plain_fits = plain_head_bytes(j) <= pt->g->smem_optin;
+  if (!fused_fits || !plain_fits) return !fused_fits;
+  const auto key = std::make_tuple(pt->g->device, j.n, j.F.nnz, j.nt, j.C);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_form.find(key);
+    if (it != g_form.end()) return it->second;
+  }
+  // small runs cannot fill the GPU with the plain form
+  bool plain = false;
+  if ((uint64_t)j.n * j.qps >= 256ull * (uint64_t)pt->g->num_sms) {
+    const TileChoice t = tune_tile(pt->g, j);
+    const float ms_fused = time_tile(pt->g, j, t, 8);
+    // time the plain form on a scratch copy
+    tamc_pt scratch;
+    scratch.inst = pt->inst;
+    scratch.g = pt->g;
+    scratch.cfg = pt->cfg;
+    scratch.cfg.meas_init = 0xffffffffu;
+    scratch.fast = new tamc_pt::FastState();
+    float ms_plain = 1e30f;
+    try {
+      fill_job(&scratch, 1, scratch.fast);
+      scratch.fast->job.meas_init = 0xffffffffu;
+      plain_setup(&scratch);
+      plain_init_energies(&scratch, true);
+      cudaEvent_t e0, e1;
+      TAMC_CUDA(cudaEventCreate(&e0));
+      TAMC_CUDA(cudaEventCreate(&e1));
+      plain_run_chunk(&scratch, 8);  // capture + warm up
+      TAMC_CUDA(cudaEventRecord(e0, pt->g->stream));
+      plain_run_chunk(&scratch, 8);
+      TAMC_CUDA(cudaEventRecord(e1, pt->g->stream));
+      TAMC_CUDA(cudaEventSynchronize(e1));
+      TAMC_CUDA(cudaEventElapsedTime(&ms_plain, e0, e1));
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    } catch (...) {
+      delete scratch.fast;
+      scratch.fast = nullptr;
+      throw;
+    }
+    delete scratch.fast;
+    scratch.fast = nullptr;
+    plain = ms_plain < ms_fused;
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_form[key] = plain;
+  return plain;
+}
+
 void fast_pt_create(tamc_pt* pt, uint64_t seed) {
   pt->fast = new tamc_pt::FastState();
   fill_job(pt, seed, pt->fast);
+  if (choose_plain(pt)) {
+    plain_setup(pt);
+    plain_init_energies(pt, true);
+    return;
+  }
   const TileChoice t = tune_tile(pt->g, pt->fast->job);
   pt->fast->T = t.T;
   pt->fast->job.csr_smem = t.csr;
@@ -225,7 +370,8 @@ void fast_pt_run(tamc_pt* pt, uint32_t sweep_end) {
   while (pt->next_sweep < sweep_end) {
     const uint32_t b = pt->next_sweep;
     const uint32_t e = std::min(sweep_end, b + pt->out.cap);
-    launch_one(pt, b, e, 0);
+    if (pt->fast->plain) plain_run_chunk(pt, e - b);
+    else launch_one(pt, b, e, 0);
     pt->m_next += count_sched(c.sample, c.meas_init, c.num_sweeps, b, e);
     pt->s_next += count_sched(c.sample_states, c.meas_init, c.num_sweeps, b, e);
     pt->next_sweep = e;
@@ -267,7 +413,8 @@ void fast_pt_set_state(tamc_pt* pt, const int8_t* spins) {
         if (src[perm[s]] < 0) W[(size_t)s * j.nw + o] |= 1u << b;
     }
   TAMC_CUDA(cudaMemcpyAsync(F->W.p, W.data(), W.size() * 4, cudaMemcpyHostToDevice, st));
-  launch_one(pt, pt->next_sweep, pt->next_sweep, 2);  // recompute energies
+  if (F->plain) plain_init_energies(pt, false);
+  else launch_one(pt, pt->next_sweep, pt->next_sweep, 2);  // recompute energies
 }
 
 void fast_pt_acceptance(tamc_pt* pt, uint32_t* acc) {
@@ -438,6 +585,7 @@ int tamc_gpu_batch_create(tamc_gpu* g, tamc_batch** out) {
   if (!g || !out) fail(TAMC_E_INVAL, "null argument");
   auto* b = new tamc_batch();
   b->g = g;
+  tamc_gpu_retain(g);
   *out = b;
   TAMC_API_END
 }
@@ -515,9 +663,11 @@ int tamc_gpu_batch_tile(tamc_batch* b, uint32_t job, uint32_t* cta_threads, uint
 int tamc_gpu_batch_destroy(tamc_batch* b) {
   TAMC_API_BEGIN
   if (!b) return TAMC_OK;
-  cudaSetDevice(b->g->device);
-  cudaStreamSynchronize(b->g->stream);
+  tamc_gpu* g = b->g;
+  cudaSetDevice(g->device);
+  cudaStreamSynchronize(g->stream);
   delete b;
+  tamc_gpu_release(g);
   TAMC_API_END
 }
 

@@ -378,7 +378,7 @@ __device__ void sweep_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t
       const uint32_t c1 = J.F.color_off[c + 1];
       for (uint32_t s = J.F.color_off[c] + tid / J.qps; s < c1; s += stride) {
         const uint4 rnd = philox4x32_10(make_uint4(s, i, qid, PTAG_SWEEP), J.key);
-        const uint32_t m = quad_update(s, shift, F, S.W, J.nw, wo, beta, rnd, acc);
+        const uint32_t m = quad_update<true>(s, shift, F, S.W, J.nw, wo, beta, rnd, acc);
         if (m) {
           atomicXor(&S.W[s * J.nw + wo], m << shift);
           if (SELF) {
@@ -543,7 +543,9 @@ __device__ void run_job(const PtJob& J, char* smem_base) {
   }
   for (uint32_t k = tid; k < J.qps; k += T) {
     const uint32_t q = k % J.qpc;
-    S.beta4[k] = make_float4(J.betas[4 * q], J.betas[4 * q + 1], J.betas[4 * q + 2], J.betas[4 * q + 3]);
+    const float L2E = 1.4426950408889634f;  // beta * log2(e) for ex2
+    S.beta4[k] = make_float4(J.betas[4 * q] * L2E, J.betas[4 * q + 1] * L2E, J.betas[4 * q + 2] * L2E,
+                             J.betas[4 * q + 3] * L2E);
   }
   const uint32_t Teff = (T / J.qps) * J.qps;
   if (J.init == 1) {
@@ -601,6 +603,177 @@ __global__ void __launch_bounds__(512, 1) k_pt_fused(const PtJob* __restrict__ j
   }
 }
 
+// ============================================================ plain form ====
+// One instance spread over the whole GPU, one launch per sweep phase:
+//   k_plain_head  (1 CTA): close the previous round (add its sweep energy sums,
+//                 measurements), then ICM and replica exchange of the next
+//                 round, with the replica words in global memory;
+//   k_plain_sweep (grid) : one launch per colour class, (site, quad) tasks
+//                 spread over all SMs, flips by atomicXor on the global words,
+//                 ΔE sums by 64-bit integer atomics (order-independent).
+// The phase functions are the fused kernel's, so both forms produce the same
+// Markov chain bit for bit; the round index and measurement counters live in
+// device memory (PlainCtl) so a captured chunk of rounds replays unchanged.
+__host__ __device__ inline size_t plain_head_smem(uint32_t n, uint32_t C, uint32_t ntp) {
+  return al16((size_t)n * 4) * 2 + al16((size_t)C * ntp * 8) * 2 + al16(32 * 4) + al16(32 * 8) * 2 +
+         al16((size_t)C * 8);
+}
+
+__global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict__ jp, PlainCtl* ctl,
+                                                       long long* acc, int mode) {
+  extern __shared__ uint4 smem_u4[];
+  const PtJob J = *jp;
+  const uint32_t tid = threadIdx.x;
+  char* base = reinterpret_cast<char*>(smem_u4);
+  Smem S{};
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    char* p = base + o;
+    o = al16(o + bytes);
+    return p;
+  };
+  S.D = (uint32_t*)take((size_t)J.n * 4);
+  S.Cl = (uint32_t*)take((size_t)J.n * 4);
+  S.Ec = (double*)take((size_t)J.C * J.ntp * 8);
+  S.Er = (double*)take((size_t)J.C * J.ntp * 8);
+  S.nneg = (uint32_t*)take(32 * 4);
+  S.dE0 = (double*)take(32 * 8);
+  S.dE1 = (double*)take(32 * 8);
+  S.Dm = (unsigned long long*)take((size_t)J.C * 8);
+  S.W = J.W;
+  const FastInst F = J.F;
+  const uint32_t CN = J.C * J.ntp;
+  long long* accq = acc + CN;
+  for (uint32_t x = tid; x < CN; x += blockDim.x) {
+    double ec = J.Ec[x], er = J.Er[x];
+    if (mode == 2) {  // initial energies from the fixed-point sums of the energy kernel
+      ec = (double)J.F.offset + (double)acc[x] * TAMC_FX_INV;
+      er = ec;
+      acc[x] = 0;
+    } else if (ctl->pending) {  // IsingSampler::sweep: energy += Σ accepted ΔE
+      ec += (double)acc[x] * TAMC_FX_INV;
+      er += (double)(acc[x] + accq[x]) * TAMC_FX_INV;
+      acc[x] = 0;
+      accq[x] = 0;
+    }
+    S.Ec[x] = ec;
+    S.Er[x] = er;
+  }
+  __syncthreads();
+  uint32_t m_cur = ctl->m_cur, s_cur = ctl->s_cur;
+  if (mode != 2 && ctl->pending) {
+    const uint32_t ip = ctl->i - 1;
+    if (ip >= J.meas_init) measure_phase(J, F, S, ip, m_cur, s_cur);
+  }
+  __syncthreads();
+  if (mode == 0) {  // start round i: ICM, then exchange; the sweeps follow
+    const uint32_t i = ctl->i;
+    if (J.icm) icm_phase(J, F, S, i);
+    exchange_phase(J, S, i);
+  }
+  for (uint32_t x = tid; x < CN; x += blockDim.x) {
+    J.Ec[x] = S.Ec[x];
+    J.Er[x] = S.Er[x];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    ctl->m_cur = m_cur;
+    ctl->s_cur = s_cur;
+    if (mode == 0) {
+      ctl->i += 1;
+      ctl->pending = 1;
+    } else {
+      ctl->pending = 0;
+    }
+    if (J.count_out) *J.count_out = *J.log.count;
+  }
+}
+
+template <bool SELF>
+__global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ jp, const PlainCtl* __restrict__ ctl,
+                                                     uint32_t color, long long* acc) {
+  extern __shared__ uint4 smem_u4[];
+  const PtJob& J = *jp;
+  const uint32_t CN = J.C * J.ntp;
+  long long* sacc = reinterpret_cast<long long*>(smem_u4);
+  long long* saccq = sacc + CN;
+  float4* b4 = reinterpret_cast<float4*>(saccq + CN + (CN & 1u));
+  for (uint32_t x = threadIdx.x; x < 2 * CN; x += blockDim.x) sacc[x] = 0;
+  const float L2E = 1.4426950408889634f;
+  for (uint32_t k = threadIdx.x; k < J.qps; k += blockDim.x) {
+    const uint32_t q = k % J.qpc;
+    b4[k] = make_float4(J.betas[4 * q] * L2E, J.betas[4 * q + 1] * L2E, J.betas[4 * q + 2] * L2E,
+                        J.betas[4 * q + 3] * L2E);
+  }
+  __syncthreads();
+  const uint32_t i = ctl->i - 1;
+  const uint32_t c0 = J.F.color_off[color], nc = J.F.color_off[color + 1] - c0;
+  const uint64_t ntask = (uint64_t)nc * J.qps;
+  const FastInst F = J.F;
+  for (uint64_t task = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; task < ntask;
+       task += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = (uint32_t)(task % J.qps);
+    const uint32_t s = c0 + (uint32_t)(task / J.qps);
+    const uint32_t ch = k / J.qpc, q = k % J.qpc;
+    const uint32_t wo = ch * J.wpc + (q >> 3), shift = 4 * (q & 7u);
+    const uint4 rnd = philox4x32_10(make_uint4(s, i, ch * 16u + q, PTAG_SWEEP), J.key);
+    Fx4 a{0, 0, 0, 0};
+    const uint32_t m = quad_update<true>(s, shift, F, J.W, J.nw, wo, b4[k], rnd, a);
+    if (m) {
+      atomicXor(&J.W[s * J.nw + wo], m << shift);
+      const uint32_t slot = ch * J.ntp + 4 * q;
+      if (m & 1u) atomicAdd((unsigned long long*)&sacc[slot + 0], (unsigned long long)a.x);
+      if (m & 2u) atomicAdd((unsigned long long*)&sacc[slot + 1], (unsigned long long)a.y);
+      if (m & 4u) atomicAdd((unsigned long long*)&sacc[slot + 2], (unsigned long long)a.z);
+      if (m & 8u) atomicAdd((unsigned long long*)&sacc[slot + 3], (unsigned long long)a.w);
+      if (SELF) {
+        const unsigned long long k2 = (unsigned long long)to_fx(2.0f * F.kd[s]);
+        for (uint32_t r = 0; r < 4; ++r)
+          if ((m >> r) & 1u) atomicAdd((unsigned long long*)&saccq[slot + r], k2);
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t x = threadIdx.x; x < 2 * CN; x += blockDim.x)
+    if (sacc[x]) atomicAdd((unsigned long long*)&acc[x], (unsigned long long)sacc[x]);
+}
+
+// Initial replicas (random, as the fused kernel's init) and their energy terms.
+__global__ void k_plain_init(const PtJob* __restrict__ jp, long long* acc, int random) {
+  const PtJob& J = *jp;
+  const uint64_t total = (uint64_t)J.n * J.nw;
+  if (random) {
+    for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+      const uint32_t s = (uint32_t)(x / J.nw), wo = (uint32_t)(x % J.nw);
+      const uint32_t ch = wo / J.wpc, w = wo % J.wpc;
+      uint32_t v = 0;
+      for (uint32_t qq = 0; qq < 8; ++qq) {
+        const uint32_t q = 8 * w + qq;
+        if (q >= J.qpc) break;
+        v |= init_nibble(philox4x32_10(make_uint4(s, 0xffffffffu, ch * 16u + q, PTAG_INIT), J.key)) << (4 * qq);
+      }
+      J.W[x] = v;
+    }
+  }
+}
+__global__ void k_plain_energy(const PtJob* __restrict__ jp, long long* acc) {
+  const PtJob& J = *jp;
+  const uint64_t ntask = (uint64_t)J.n * J.qps;
+  for (uint64_t task = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; task < ntask;
+       task += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = (uint32_t)(task % J.qps), s = (uint32_t)(task / J.qps);
+    const uint32_t ch = k / J.qpc, q = k % J.qpc;
+    const uint32_t wo = ch * J.wpc + (q >> 3), shift = 4 * (q & 7u);
+    const float4 e = energy_terms4(s, shift, J.F, J.W, J.nw, wo);
+    const uint32_t slot = ch * J.ntp + 4 * q;
+    atomicAdd((unsigned long long*)&acc[slot + 0], (unsigned long long)to_fx(e.x));
+    atomicAdd((unsigned long long*)&acc[slot + 1], (unsigned long long)to_fx(e.y));
+    atomicAdd((unsigned long long*)&acc[slot + 2], (unsigned long long)to_fx(e.z));
+    atomicAdd((unsigned long long*)&acc[slot + 3], (unsigned long long)to_fx(e.w));
+  }
+}
+
 }  // namespace
 
 size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem) {
@@ -612,6 +785,35 @@ int fused_blocks_per_sm(uint32_t T, size_t smem) {
   int nb = 0;
   TAMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pt_fused, (int)T, smem));
   return nb;
+}
+
+size_t plain_head_bytes(const PtJob& j) { return plain_head_smem(j.n, j.C, j.ntp); }
+
+void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem) {
+  TAMC_CUDA(cudaFuncSetAttribute(k_plain_head, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_plain_head<<<1, 1024, smem, st>>>(d_job, ctl, acc, mode);
+  TAMC_CUDA(cudaGetLastError());
+}
+
+void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, uint32_t color,
+                        uint32_t ntask, long long* acc, uint32_t grid_cap) {
+  const uint32_t T = 256;
+  const uint32_t grid = std::max(1u, std::min(grid_cap, (ntask + T - 1) / T));
+  const size_t smem = (size_t)(2 * j.C * j.ntp + 2) * 8 + (size_t)j.qps * 16;
+  if (j.self_loops) {
+    TAMC_CUDA(cudaFuncSetAttribute(k_plain_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plain_sweep<true><<<grid, T, smem, st>>>(d_job, ctl, color, acc);
+  } else {
+    TAMC_CUDA(cudaFuncSetAttribute(k_plain_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plain_sweep<false><<<grid, T, smem, st>>>(d_job, ctl, color, acc);
+  }
+  TAMC_CUDA(cudaGetLastError());
+}
+
+void plain_launch_init(cudaStream_t st, const PtJob* d_job, long long* acc, int random, uint32_t grid) {
+  if (random) k_plain_init<<<grid, 256, 0, st>>>(d_job, acc, 1);
+  k_plain_energy<<<grid, 256, 0, st>>>(d_job, acc);
+  TAMC_CUDA(cudaGetLastError());
 }
 
 void fused_launch(cudaStream_t st, const PtJob* d_jobs, uint32_t njobs, uint32_t* ctr, uint32_t grid, uint32_t T,

@@ -40,6 +40,20 @@ int fused_blocks_per_sm(uint32_t T, size_t smem);
 void fused_launch(cudaStream_t st, const PtJob* d_jobs, uint32_t njobs, uint32_t* ctr, uint32_t grid,
                   uint32_t T, size_t smem);
 
+// Plain form (one instance over the whole GPU, one launch per sweep phase).
+struct PlainCtl {
+  uint32_t i;        // next round to start
+  uint32_t m_cur;    // next measurement index
+  uint32_t s_cur;    // next state-snapshot index
+  uint32_t pending;  // the sweeps of round i-1 ran; their sums and measurements are pending
+};
+size_t plain_head_bytes(const PtJob& j);
+// mode 0: close the previous round and start round ctl->i; 1: only close; 2: set initial energies
+void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem);
+void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, uint32_t color,
+                        uint32_t ntask, long long* acc, uint32_t grid_cap);
+void plain_launch_init(cudaStream_t st, const PtJob* d_job, long long* acc, int random, uint32_t grid);
+
 // tamc_pt glue (single-instance handle in fast mode)
 void fast_pt_create(tamc_pt* pt, uint64_t seed);
 void fast_pt_run(tamc_pt* pt, uint32_t sweep_end);

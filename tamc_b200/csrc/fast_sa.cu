@@ -11,12 +11,16 @@
 #include "fast_common.cuh"
 #include "fast_sa.cuh"
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 namespace tamc {
 
 namespace {
 
 template <int NQ, bool SMEM>
-__global__ void __launch_bounds__(512) k_sa_fast(SaFastArgs a) {
+__global__ void __launch_bounds__(1024) k_sa_fast(SaFastArgs a) {
   extern __shared__ uint4 smem_u4[];
   constexpr uint32_t G = 4 * NQ;
   const uint32_t T = blockDim.x, tid = threadIdx.x;
@@ -54,15 +58,15 @@ __global__ void __launch_bounds__(512) k_sa_fast(SaFastArgs a) {
   const uint32_t shift = 4 * q;
   const uint32_t qid = (r0 >> 2) + q;
   const uint32_t stride = T / NQ;
-  Fx4 acc{0, 0, 0, 0};
+  Fx4 acc{0, 0, 0, 0};  // unused: SA energies are computed once at the end
   for (uint32_t sw = 0; sw < a.nbeta; ++sw) {
-    const float b = a.betas[sw];
+    const float b = a.betas[sw] * 1.4426950408889634f;  // beta * log2(e)
     const float4 beta = make_float4(b, b, b, b);
     for (uint32_t c = 0; c < F.ncolors; ++c) {
       const uint32_t c1 = a.F.color_off[c + 1];
       for (uint32_t s = a.F.color_off[c] + tid / NQ; s < c1; s += stride) {
         const uint4 rnd = philox4x32_10(make_uint4(s, sw, qid, PTAG_SWEEP), key);
-        const uint32_t m = quad_update(s, shift, F, W, 1, 0, beta, rnd, acc);
+        const uint32_t m = quad_update<false>(s, shift, F, W, 1, 0, beta, rnd, acc);
         if (m) {
           if (NQ == 1) W[s] ^= m;
           else atomicXor(&W[s], m << shift);
@@ -113,6 +117,20 @@ __global__ void __launch_bounds__(512) k_sa_fast(SaFastArgs a) {
   }
 }
 
+// words [ceil(R/32)][n] (bit r%32 = replica r) -> packed [R][ceil(n/8)] bytes
+// (bit i%8 of byte i/8 = site i), the IsingState::write_to_bytes layout
+// (src/ising.rs:102-115).  One thread per output byte.
+__global__ void k_pack_states(const uint32_t* __restrict__ words, uint32_t n, uint32_t R, uint8_t* __restrict__ out) {
+  const uint32_t nb = (n + 7) / 8;
+  const uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= (uint64_t)R * nb) return;
+  const uint32_t r = (uint32_t)(x / nb), b = (uint32_t)(x % nb);
+  const uint32_t* w = words + (size_t)(r >> 5) * n;
+  uint32_t v = 0;
+  for (uint32_t k = 0; k < 8 && 8 * b + k < n; ++k) v |= ((w[8 * b + k] >> (r & 31u)) & 1u) << k;
+  out[x] = (uint8_t)v;
+}
+
 template <int NQ, bool SMEM>
 void launch_t(cudaStream_t st, const SaFastArgs& a, uint32_t ncta, uint32_t T, size_t smem) {
   auto k = k_sa_fast<NQ, SMEM>;
@@ -128,23 +146,111 @@ size_t sa_fast_smem(const FastInst& F, uint32_t nq, uint32_t T, bool smem_csr) {
   return ((words + 1) / 2 + 1) * 8 + (size_t)(T / 32) * nq * 4 * 8 + 16;
 }
 
-SaTile sa_fast_choose(const tamc_gpu* g, const FastInst& F, uint32_t R) {
+void sa_pack_states(cudaStream_t st, const uint32_t* words, uint32_t n, uint32_t R, uint8_t* out) {
+  const uint64_t total = (uint64_t)R * ((n + 7) / 8);
+  if (!total) return;
+  k_pack_states<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(words, n, R, out);
+  TAMC_CUDA(cudaGetLastError());
+}
+
+// Heuristic tile: the smallest replica group (quads per CTA) that still gives
+// every SM at least one CTA.
+static SaTile heuristic(const tamc_gpu* g, const FastInst& F, uint32_t R) {
   SaTile t;
   t.T = 512;
-  t.smem_csr = sa_fast_smem(F, 8, t.T, true) <= g->smem_optin;
-  // smallest replica group that still gives every SM a CTA
+  t.smem_csr = sa_fast_smem(F, 8, 1024, true) <= g->smem_optin;
   t.nq = 8;
   for (uint32_t nq : {1u, 2u, 4u, 8u}) {
     const uint32_t ncta = (R + 4 * nq - 1) / (4 * nq);
     if (ncta <= (uint32_t)g->num_sms) { t.nq = nq; break; }
   }
+  t.smem = sa_fast_smem(F, t.nq, t.T, t.smem_csr);
+  return t;
+}
+
+// Autotuner: times a short anneal (a few sweeps) of each candidate tile --
+// replicas per CTA (4*nq) x CTA size -- on scratch buffers the first time a
+// (device, n, nnz, R) shape is seen, and caches the fastest.  The choice does
+// not change results: spins depend only on (seed, site, sweep, replica) and
+// energies are fixed-point sums.
+static std::mutex g_sa_mu;
+static std::map<std::tuple<int, uint32_t, uint32_t, uint32_t>, SaTile> g_sa_tune;
+
+SaTile sa_fast_choose(tamc_gpu* g, const FastInst& F, uint32_t R) {
+  const auto key = std::make_tuple(g->device, F.n, F.nnz, R);
+  {
+    std::lock_guard<std::mutex> lk(g_sa_mu);
+    auto it = g_sa_tune.find(key);
+    if (it != g_sa_tune.end()) return it->second;
+  }
+  SaTile best = heuristic(g, F, R);
+  const char* env = getenv("TAMC_AUTOTUNE");
+  if ((!env || env[0] != '0') && R >= 64) {
+    const uint32_t nb = 8;
+    float* d_b = nullptr;
+    float* d_e = nullptr;
+    uint32_t* d_w = nullptr;
+    TAMC_CUDA(cudaMalloc((void**)&d_b, nb * 4));
+    TAMC_CUDA(cudaMalloc((void**)&d_e, (size_t)R * 4));
+    TAMC_CUDA(cudaMalloc((void**)&d_w, (size_t)((R + 31) / 32) * F.n * 4));
+    std::vector<float> hb(nb, 1.0f);
+    TAMC_CUDA(cudaMemcpy(d_b, hb.data(), nb * 4, cudaMemcpyHostToDevice));
+    cudaEvent_t e0, e1;
+    TAMC_CUDA(cudaEventCreate(&e0));
+    TAMC_CUDA(cudaEventCreate(&e1));
+    float best_ms = 1e30f;
+    for (uint32_t nq : {1u, 2u, 4u, 8u}) {
+      for (uint32_t T : {256u, 512u, 1024u}) {
+        SaTile t;
+        t.nq = nq;
+        t.T = T;
+        t.smem_csr = best.smem_csr;
+        t.smem = sa_fast_smem(F, nq, T, t.smem_csr);
+        if (t.smem > g->smem_optin) continue;
+        const uint32_t ncta = (R + 4 * nq - 1) / (4 * nq);
+        if (ncta * 4 < (uint32_t)g->num_sms && nq > 1) continue;  // too few CTAs to fill the GPU
+        SaFastArgs a;
+        a.F = F;
+        a.betas = d_b;
+        a.nbeta = nb;
+        a.key = make_uint2(1u, 2u);
+        a.R = R;
+        a.init_words = nullptr;
+        a.words_out = d_w;
+        a.energies_out = d_e;
+        float ms = 0.0f;
+        for (int rep = 0; rep < 2; ++rep) {
+          TAMC_CUDA(cudaMemsetAsync(d_w, 0, (size_t)((R + 31) / 32) * F.n * 4, g->stream));
+          TAMC_CUDA(cudaEventRecord(e0, g->stream));
+          sa_fast_launch(g->stream, a, t);
+          TAMC_CUDA(cudaEventRecord(e1, g->stream));
+          g->count();
+          TAMC_CUDA(cudaEventSynchronize(e1));
+          TAMC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        }
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = t;
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d_b);
+    cudaFree(d_e);
+    cudaFree(d_w);
+  }
   if (const char* e = getenv("TAMC_SA_NQ")) {
     const int v = atoi(e);
-    if (v == 1 || v == 2 || v == 4 || v == 8) t.nq = (uint32_t)v;
+    if (v == 1 || v == 2 || v == 4 || v == 8) {
+      best.nq = (uint32_t)v;
+      best.smem = sa_fast_smem(F, best.nq, best.T, best.smem_csr);
+    }
   }
-  t.smem = sa_fast_smem(F, t.nq, t.T, t.smem_csr);
-  if (t.smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the fast SA kernel");
-  return t;
+  if (best.smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the fast SA kernel");
+  std::lock_guard<std::mutex> lk(g_sa_mu);
+  g_sa_tune[key] = best;
+  return best;
 }
 
 void sa_fast_launch(cudaStream_t st, const SaFastArgs& a, const SaTile& t) {

@@ -22,7 +22,9 @@ struct SaTile {
   size_t smem = 0;
 };
 
-SaTile sa_fast_choose(const tamc_gpu* g, const FastInst& F, uint32_t R);
+SaTile sa_fast_choose(tamc_gpu* g, const FastInst& F, uint32_t R);
+// Device-side conversion of SA words to the reference's packed byte layout.
+void sa_pack_states(cudaStream_t st, const uint32_t* words, uint32_t n, uint32_t R, uint8_t* out);
 void sa_fast_launch(cudaStream_t st, const SaFastArgs& a, const SaTile& t);
 
 }  // namespace tamc

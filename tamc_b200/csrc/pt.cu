@@ -244,6 +244,7 @@ int tamc_gpu_pt_create(tamc_inst* inst, const tamc_pt_params* p, uint64_t seed, 
   if (mode != TAMC_MODE_REF && mode != TAMC_MODE_FAST) fail(TAMC_E_INVAL, "unknown mode");
   TAMC_CUDA(cudaSetDevice(inst->g->device));
   auto* pt = new tamc_pt();
+  tamc_inst_retain(inst);
   try {
     pt->inst = inst;
     pt->g = inst->g;
@@ -256,6 +257,7 @@ int tamc_gpu_pt_create(tamc_inst* inst, const tamc_pt_params* p, uint64_t seed, 
   } catch (...) {
     if (pt->fast) fast_pt_destroy(pt);
     delete pt;
+    tamc_inst_release(inst);
     throw;
   }
   *out = pt;
@@ -436,7 +438,9 @@ int tamc_gpu_pt_destroy(tamc_pt* pt) {
   cudaSetDevice(pt->g->device);
   cudaStreamSynchronize(pt->g->stream);
   if (pt->fast) fast_pt_destroy(pt);
+  tamc_inst* inst = pt->inst;
   delete pt;
+  tamc_inst_release(inst);
   TAMC_API_END
 }
 

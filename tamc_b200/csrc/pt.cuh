@@ -106,4 +106,5 @@ struct tamc_pt {
   // fast-mode state lives behind an opaque pointer (fast_pt.cu)
   struct FastState;
   FastState* fast = nullptr;
+  bool fast_plain() const;  // the run uses the all-SM plain form
 };

@@ -104,10 +104,11 @@ int tamc_gpu_sa_run(tamc_inst* inst, const float* betas, uint32_t nbeta, uint32_
       for (uint32_t i = 0; i < n; ++i)
         if (spins[(size_t)r * n + i] <= 0) packed[(size_t)r * nbytes + i / 8] |= (uint8_t)(1u << (i % 8));
   } else if (mode == TAMC_MODE_FAST) {
+    // device buffers are cached on the instance and reused across calls
+    SaScratch& sc = inst->sa_scratch;
     const uint32_t nw = (R + 31) / 32;
-    DBuf<uint32_t> d_words((size_t)nw * n);
-    DBuf<float> d_e(R);
-    TAMC_CUDA(cudaMemsetAsync(d_words.p, 0, (size_t)nw * n * 4, st));
+    sc.ensure((size_t)nw * n, R, (size_t)R * nbytes);
+    TAMC_CUDA(cudaMemsetAsync(sc.words, 0, (size_t)nw * n * 4, st));
     SaFastArgs a;
     a.F = make_fast_inst(inst);
     a.betas = d_betas.p;
@@ -115,20 +116,17 @@ int tamc_gpu_sa_run(tamc_inst* inst, const float* betas, uint32_t nbeta, uint32_
     a.key = philox_key(seed);
     a.R = R;
     a.init_words = nullptr;
-    a.words_out = d_words.p;
-    a.energies_out = d_e.p;
+    a.words_out = sc.words;
+    a.energies_out = sc.energies;
     const SaTile t = sa_fast_choose(g, a.F, R);
     sa_fast_launch(st, a, t);
-    g->count();
-    std::vector<uint32_t> words((size_t)nw * n);
-    TAMC_CUDA(cudaMemcpyAsync(words.data(), d_words.p, words.size() * 4, cudaMemcpyDeviceToHost, st));
-    TAMC_CUDA(cudaMemcpyAsync(e.data(), d_e.p, R * 4, cudaMemcpyDeviceToHost, st));
+    sa_pack_states(st, sc.words, n, R, sc.packed);
+    g->count(2);
+    if (energies_out) TAMC_CUDA(cudaMemcpyAsync(energies_out, sc.energies, R * 4, cudaMemcpyDeviceToHost, st));
+    if (packed_out)
+      TAMC_CUDA(cudaMemcpyAsync(packed_out, sc.packed, (size_t)R * nbytes, cudaMemcpyDeviceToHost, st));
     TAMC_CUDA(cudaStreamSynchronize(st));
-    for (uint32_t r = 0; r < R; ++r) {
-      const uint32_t* w = words.data() + (size_t)(r / 32) * n;
-      for (uint32_t i = 0; i < n; ++i)
-        if ((w[i] >> (r % 32)) & 1u) packed[(size_t)r * nbytes + i / 8] |= (uint8_t)(1u << (i % 8));
-    }
+    return TAMC_OK;
   } else {
     fail(TAMC_E_INVAL, "unknown mode");
   }

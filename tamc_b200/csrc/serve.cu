@@ -18,6 +18,7 @@
 #include "fast_pt.cuh"
 
 namespace tamc {
+extern thread_local bool g_no_autotune;
 struct ChunkRunner;
 void chunk_run(ChunkRunner* r, tamc_gpu* g, std::vector<tamc_pt*>& act, uint32_t chunk);
 ChunkRunner* chunk_runner_new();
@@ -108,6 +109,7 @@ int tamc_serve_create(tamc_gpu* g, uint64_t hbm_budget_bytes, uint32_t max_activ
   if (!max_active || !chunk_sweeps) fail(TAMC_E_INVAL, "max_active and chunk_sweeps must be > 0");
   auto* s = new tamc_server();
   s->g = g;
+  tamc_gpu_retain(g);
   s->budget = hbm_budget_bytes;
   s->max_active = max_active;
   s->chunk = std::min(chunk_sweeps, 1024u);
@@ -153,8 +155,11 @@ int tamc_serve_step(tamc_server* s, uint32_t* active, uint32_t* queued) {
     s->queue.pop_front();
     int rc = tamc_gpu_instance_upload(s->g, r->h, &r->dinst);
     if (rc != TAMC_OK) fail(rc, tamc_last_error());
+    g_no_autotune = true;
     rc = tamc_gpu_pt_create(r->dinst, &r->p, r->seed, TAMC_MODE_FAST, &r->pt);
+    g_no_autotune = false;
     if (rc != TAMC_OK) fail(rc, tamc_last_error());
+    if (r->pt->fast && r->pt->fast_plain()) fail(TAMC_E_UNSUPPORTED, "request too large for the fused PT kernel");
     r->state = 1;
     s->used += r->footprint;
     s->active.push_back(r);
@@ -208,9 +213,11 @@ int tamc_serve_state(tamc_server* s, uint64_t request_id, int8_t* spins, float* 
 int tamc_serve_destroy(tamc_server* s) {
   TAMC_API_BEGIN
   if (!s) return TAMC_OK;
-  cudaSetDevice(s->g->device);
-  cudaStreamSynchronize(s->g->stream);
+  tamc_gpu* g = s->g;
+  cudaSetDevice(g->device);
+  cudaStreamSynchronize(g->stream);
   delete s;
+  tamc_gpu_release(g);
   TAMC_API_END
 }
 

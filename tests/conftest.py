@@ -31,9 +31,9 @@ def tb():
 
 @pytest.fixture(scope="session")
 def gpu(tb):
-    g = tb.Gpu(0)
-    yield g
-    g.close()
+    # handles are reference-counted in the library: objects created from this
+    # context keep it alive until they are collected
+    return tb.Gpu(0)
 
 
 def load_golden(name):

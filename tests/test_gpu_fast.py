@@ -253,3 +253,36 @@ def test_server_admission_and_target_energy(tb, gpu):
     with pytest.raises(tb.TamcError) as e:
         tiny.submit(h, p, 1)
     assert e.value.code == -9
+
+
+@pytest.mark.parametrize("kind", ["2d_gauss", "3d_gauss_64", "qubo"])
+def test_pt_fused_and_plain_forms_identical(tb, po, gpu, monkeypatch, kind):
+    """The single-CTA fused form and the all-SM plain form run the same chain."""
+    if kind == "2d_gauss":
+        text, qubo, nt, C = gi.lattice(8, 2, "gauss", 3), False, 16, 2
+    elif kind == "3d_gauss_64":
+        text, qubo, nt, C = gi.lattice(6, 3, "gauss", 4), False, 64, 2
+    else:
+        text, qubo, nt, C = gi.qubo_er(150, 5, 6), True, 12, 4
+    b = po.geometric_betas(0.2, 3.0, nt)
+    p = _pt(tb, 90, b, nt // 2, C, 8, 7, 11, 0)
+    h = tb.HostInstance.parse(text, qubo=qubo)
+    if kind == "3d_gauss_64":
+        h.add_suscept(gi.fourier_weights(6, 3, 0))
+    d = gpu.upload(h)
+    out = []
+    for form in ("fused", "plain"):
+        monkeypatch.setenv("TAMC_PT_FORM", form)
+        r = tb.PtRun(d, p, 9).run().sync()
+        ts = r.samples()
+        out.append((r.state(), r.gs(), np.array(ts.e), np.array(ts.q), np.array(ts.suscept), np.array(ts.samples),
+                    r.acceptance(), r.round_trips()))
+    (s0, e0), g0 = out[0][0], out[0][1]
+    (s1, e1), g1 = out[1][0], out[1][1]
+    assert np.array_equal(s0, s1) and np.array_equal(e0, e1)
+    for a, c in zip(g0, g1):
+        assert np.array_equal(a, c)
+    for a, c in zip(out[0][2:7], out[1][2:7]):
+        assert np.array_equal(a, c)
+    for a, c in zip(out[0][7], out[1][7]):
+        assert np.array_equal(a, c)
