@@ -173,6 +173,10 @@ int tamc_gpu_pt_samples_dims(tamc_pt* pt, uint32_t* M, uint32_t* S, uint32_t* Z,
 /* e [nt][M*C], q [nt][M*C/2], suscept [nt][nchi][M*C/2], samples [Z][S*C][ceil(n/8)];
  * any pointer may be NULL to skip it. */
 int tamc_gpu_pt_samples(tamc_pt* pt, float* e, int32_t* q, float* suscept, uint8_t* samples);
+/* Fast mode with TAMC_PHASE_PROF=1 in the environment at creation: SM cycles
+ * spent per round phase (ICM scan, ICM cluster growth, ICM apply, exchange,
+ * sweep, measurement, other), summed over rounds; zeros otherwise. cycles[7]. */
+int tamc_gpu_pt_phase_cycles(tamc_pt* pt, uint64_t* cycles);
 /* Wall time of the sweep loop in microseconds (the reference's `timing`). */
 double tamc_gpu_pt_timing_us(tamc_pt* pt);
 int tamc_gpu_pt_destroy(tamc_pt* pt);

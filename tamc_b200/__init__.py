@@ -98,6 +98,7 @@ _SIGS = {
     "tamc_gpu_pt_samples_dims": (C.c_int, [vp, u32p, u32p, u32p, u32p]),
     "tamc_gpu_pt_samples": (C.c_int, [vp, f32p, i32p, f32p, u8p]),
     "tamc_gpu_pt_timing_us": (C.c_double, [vp]),
+    "tamc_gpu_pt_phase_cycles": (C.c_int, [vp, u64p]),
     "tamc_gpu_pt_destroy": (C.c_int, [vp]),
     "tamc_gpu_sa_run": (C.c_int, [vp, f32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_int, f32p, u8p,
                                   u32p]),
@@ -428,6 +429,14 @@ class PtRun:
     @property
     def timing_us(self) -> float:
         return lib().tamc_gpu_pt_timing_us(self.h)
+
+    PHASES = ("icm_scan", "icm_grow", "icm_apply", "exchange", "sweep", "measure", "other")
+
+    def phase_cycles(self) -> dict:
+        """Cycles per round phase (fast mode, TAMC_PHASE_PROF=1 at creation)."""
+        a = np.zeros(7, np.uint64)
+        _check(lib().tamc_gpu_pt_phase_cycles(self.h, _p(a, u64p)))
+        return dict(zip(self.PHASES, a.tolist()))
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -35,6 +35,30 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
   return c;
 }
 
+// The same generator with the ten round keys computed once (they depend only
+// on the seed): saves the two key additions per round in hot loops.
+struct PhiloxKeys {
+  uint32_t x[10], y[10];
+};
+__host__ __device__ __forceinline__ PhiloxKeys philox_schedule(uint2 k) {
+  PhiloxKeys K;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    K.x[r] = k.x + (uint32_t)r * 0x9E3779B9u;
+    K.y[r] = k.y + (uint32_t)r * 0xBB67AE85u;
+  }
+  return K;
+}
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys& K) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ K.x[r], lo1, hi0 ^ c.w ^ K.y[r], lo0);
+  }
+  return c;
+}
+
 // Counter tags that keep the Philox streams of different uses disjoint.
 enum : uint32_t {
   PTAG_SWEEP = 0x5357u,   // Metropolis uniforms

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -26,9 +27,12 @@ struct tamc_pt::FastState {
   bool plain = false;
   tamc::DBuf<tamc::PlainCtl> ctl;
   tamc::DBuf<long long> eacc;  // fixed-point sweep sums (2 x C x ntp)
+  tamc::DBuf<long long> icm_dE;     // fixed-point ICM energy changes (C x ntp)
+  tamc::DBuf<uint32_t> icm_valid;   // caches invalidated by ICM (C x ntp)
   size_t head_smem = 0;
   uint32_t grid_cap = 0;
   std::map<uint32_t, cudaGraphExec_t> graphs;  // captured chunks of K rounds
+  tamc::DBuf<unsigned long long> prof;          // per-phase cycles (TAMC_PHASE_PROF=1)
   ~FastState() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
   }
@@ -135,6 +139,8 @@ static TileChoice tune_tile(tamc_gpu* g, const PtJob& j) {
       }
     }
   }
+  if (getenv("TAMC_DEBUG"))
+    fprintf(stderr, "[tamc] PT fused tile n=%u nt=%u C=%u: threads=%u csr_smem=%d\n", j.n, j.nt, j.C, best.T, (int)best.csr);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = best;
   return best;
@@ -200,7 +206,27 @@ static void fill_job(tamc_pt* pt, uint64_t seed, tamc_pt::FastState* F) {
   j.out = pt->out.meas(c);
   j.log = pt->out.log();
   j.count_out = nullptr;
+  j.prof = nullptr;
+  if (const char* e = getenv("TAMC_PHASE_PROF")) {
+    if (e[0] == '1') {
+      F->prof.alloc(PHASE_N);
+      F->prof.zero(st);
+      j.prof = F->prof.p;
+    }
+  }
   j.cost = (uint64_t)c.num_sweeps * j.n * j.C * j.ntp;
+  // ICM slots labelled together: all active slots of a word if their label
+  // arrays fit (aiming at <= 110 KB of shared memory so two CTAs can share an
+  // SM), else fewer
+  uint32_t active = 0;
+  for (uint32_t w = 0; w < j.wpc; ++w) {
+    uint32_t a = 0;
+    for (uint32_t b = 0; b < 32; ++b) a += (32 * w + b >= j.lo && 32 * w + b < j.nt);
+    active = std::max(active, a);
+  }
+  const size_t budget = std::min<size_t>(pt->g->smem_optin, 110 * 1024);
+  j.icm_group = std::max(1u, active);
+  while (j.icm_group > 1 && fused_smem_bytes(j, 512, false) > budget) --j.icm_group;
 }
 
 static uint32_t count_sched(int64_t period, uint32_t meas_init, uint32_t num_sweeps, uint32_t a, uint32_t b) {
@@ -234,7 +260,9 @@ static void plain_enqueue_rounds(tamc_pt* pt, uint32_t K) {
   cudaStream_t st = pt->g->stream;
   const auto& off = pt->inst->color_off;
   for (uint32_t r = 0; r < K; ++r) {
-    plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 0, F->head_smem);
+    plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem);
+    plain_launch_icm(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p);
+    plain_launch_exch(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p);
     for (uint32_t c = 0; c + 1 < off.size(); ++c)
       plain_launch_sweep(st, j, F->d_job.p, F->ctl.p, c, (off[c + 1] - off[c]) * j.qps, F->eacc.p, F->grid_cap);
   }
@@ -256,7 +284,7 @@ static void plain_run_chunk(tamc_pt* pt, uint32_t K) {
     it = F->graphs.emplace(K, exec).first;
   }
   TAMC_CUDA(cudaGraphLaunch(it->second, st));
-  pt->g->count((uint64_t)K * (1 + pt->inst->ncolors) + 1);
+  pt->g->count((uint64_t)K * (3 + pt->inst->ncolors) + 1);
 }
 
 static void plain_setup(tamc_pt* pt) {
@@ -271,6 +299,10 @@ static void plain_setup(tamc_pt* pt) {
   F->ctl.zero(st);
   F->eacc.alloc(2 * (size_t)j.C * j.ntp);
   F->eacc.zero(st);
+  F->icm_dE.alloc((size_t)j.C * j.ntp);
+  F->icm_valid.alloc((size_t)j.C * j.ntp);
+  F->icm_valid.zero(st);
+  if (plain_icm_bytes(j) > pt->g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the plain ICM kernel");
   j.init = 0;
   j.count_out = nullptr;
   TAMC_CUDA(cudaMemcpyAsync(F->d_job.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
@@ -344,6 +376,7 @@ static bool choose_plain(tamc_pt* pt) {
     scratch.fast = nullptr;
     plain = ms_plain < ms_fused;
   }
+  if (getenv("TAMC_DEBUG")) fprintf(stderr, "[tamc] PT form n=%u nt=%u C=%u: %s\n", j.n, j.nt, j.C, plain ? "plain" : "fused");
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_form[key] = plain;
   return plain;
@@ -430,6 +463,14 @@ void fast_pt_round_trips(tamc_pt* pt, uint8_t* tags, uint32_t* round_trips, uint
   if (round_trips) TAMC_CUDA(cudaMemcpyAsync(round_trips, F->rtrips.p, F->rtrips.n * 4, cudaMemcpyDeviceToHost, st));
   if (dhist) TAMC_CUDA(cudaMemcpyAsync(dhist, F->dhist.p, F->dhist.n * 4, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
+}
+
+void fast_pt_phase_cycles(tamc_pt* pt, uint64_t* out) {
+  auto* F = pt->fast;
+  for (int k = 0; k < PHASE_N; ++k) out[k] = 0;
+  if (!F || !F->prof.p) return;
+  TAMC_CUDA(cudaMemcpyAsync(out, F->prof.p, PHASE_N * 8, cudaMemcpyDeviceToHost, pt->g->stream));
+  TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
 }
 
 void fast_pt_destroy(tamc_pt* pt) {

@@ -26,6 +26,8 @@
 //     measurements and bit-packed state snapshots (src/pt.rs:167-226, 542-583).
 #include "fast_pt.cuh"
 
+#include <numeric>
+
 namespace tamc {
 namespace {
 
@@ -35,20 +37,46 @@ __device__ __forceinline__ uint64_t bitperm(uint64_t v, uint64_t D) {
   return ((v >> 1) & D) | (((v & S) + D) & E) | (v & ~(D | (D << 1)));
 }
 
+// Phase cycle accounting (thread 0, after the phase's closing barrier).
+struct PhaseClock {
+  unsigned long long* out;
+  long long t;
+  __device__ __forceinline__ void start(unsigned long long* o) {
+    out = o;
+    if (out && threadIdx.x == 0) t = clock64();
+  }
+  __device__ __forceinline__ void lap(int phase) {
+    if (out && threadIdx.x == 0) {
+      const long long now = clock64();
+      atomicAdd(&out[phase], (unsigned long long)(now - t));
+      t = now;
+    }
+  }
+};
+
 __device__ __forceinline__ float u24(uint32_t r) { return (float)(r >> 8) * (1.0f / 16777216.0f); }
+
+// Scratch of one ICM group (all in shared memory).
+struct IcmScratch {
+  uint32_t* D;     // [n] disagreement bits of the group's slots
+  uint32_t* Cl;    // [n] cluster bits
+  uint32_t* L;     // [G][n] union-find labels, G = popcount of the group mask
+  uint32_t* cnt;   // [32] q<0 counts per bit
+  uint32_t* seed;  // [32] seed site per bit
+  uint32_t* gidx;  // [32] label-array index per bit
+  unsigned long long* dE;  // [2][32] fixed-point energy change per chain and bit
+  uint32_t* red;   // [32] block reduction scratch
+  long long* part; // [32 warps][2] per-warp partial sums
+};
 
 struct Smem {
   uint32_t* W;
-  uint32_t* D;
-  uint32_t* Cl;
+  IcmScratch X;
   double* Ec;
   double* Er;
   float4* beta4;
   float4* red;
   float4* redq;
-  uint32_t* nneg;
-  double* dE0;
-  double* dE1;
   unsigned long long* Dm;
   uint32_t* rp;
   float* bias;
@@ -57,25 +85,51 @@ struct Smem {
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
+__host__ __device__ inline size_t carve_icm(IcmScratch* X, char* base, size_t o, uint32_t n, uint32_t G) {
+  auto take = [&](size_t bytes) {
+    char* p = base ? base + o : nullptr;
+    o = al16(o + bytes);
+    return p;
+  };
+  char* D = take((size_t)n * 4);
+  char* Cl = take((size_t)n * 4);
+  char* L = take((size_t)G * n * 4);
+  char* cnt = take(32 * 4);
+  char* seed = take(32 * 4);
+  char* gidx = take(32 * 4);
+  char* dE = take(64 * 8);
+  char* red = take(32 * 4);
+  char* part = take(64 * 8);
+  if (X) {
+    X->D = (uint32_t*)D;
+    X->Cl = (uint32_t*)Cl;
+    X->L = (uint32_t*)L;
+    X->cnt = (uint32_t*)cnt;
+    X->seed = (uint32_t*)seed;
+    X->gidx = (uint32_t*)gidx;
+    X->dE = (unsigned long long*)dE;
+    X->red = (uint32_t*)red;
+    X->part = (long long*)part;
+  }
+  return o;
+}
+
 __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uint32_t nw, uint32_t C, uint32_t ntp,
-                                            uint32_t qps, uint32_t T, uint32_t nnz, bool csr) {
+                                            uint32_t qps, uint32_t T, uint32_t nnz, bool csr, uint32_t G) {
   size_t o = 0;
   auto take = [&](size_t bytes) {
-    char* p = base + o;
+    char* p = base ? base + o : nullptr;
     o = al16(o + bytes);
     return p;
   };
   char* W = take((size_t)n * nw * 4);
-  char* D = take((size_t)n * 4);
-  char* Cl = take((size_t)n * 4);
+  IcmScratch X;
+  o = carve_icm(&X, base, o, n, G);
   char* Ec = take((size_t)C * ntp * 8);
   char* Er = take((size_t)C * ntp * 8);
   char* b4 = take((size_t)qps * 16);
   char* red = take((size_t)T * 16);
   char* redq = take((size_t)T * 16);
-  char* nneg = take(32 * 4);
-  char* dE0 = take(32 * 8);
-  char* dE1 = take(32 * 8);
   char* Dm = take((size_t)C * 8);
   char* rp = nullptr;
   char* bias = nullptr;
@@ -87,16 +141,12 @@ __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uin
   }
   if (S) {
     S->W = (uint32_t*)W;
-    S->D = (uint32_t*)D;
-    S->Cl = (uint32_t*)Cl;
+    S->X = X;
     S->Ec = (double*)Ec;
     S->Er = (double*)Er;
     S->beta4 = (float4*)b4;
     S->red = (float4*)red;
     S->redq = (float4*)redq;
-    S->nneg = (uint32_t*)nneg;
-    S->dE0 = (double*)dE0;
-    S->dE1 = (double*)dE1;
     S->Dm = (unsigned long long*)Dm;
     S->rp = (uint32_t*)rp;
     S->bias = (float*)bias;
@@ -142,9 +192,259 @@ __device__ void full_energies(const PtJob& J, const FastInst& F, Smem& S, uint32
   __syncthreads();
 }
 
-__device__ void icm_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i) {
+// ------------------------------------------------------------------ ICM ----
+// Union-find connected-component labelling on the subgraph where the two
+// replicas of a slot disagree.  Labels are site indices; a root is its own
+// label and every label points to a smaller-or-equal index, so `uf_find`
+// terminates and concurrent hooking (atomicMin of the larger root onto the
+// smaller) is lock-free.
+// find with path halving: every visited node is re-pointed at its
+// grandparent.  A plain store is enough: the new parent is an ancestor of the
+// node, and a concurrent atomicMin hook that such a store overwrites is
+// re-linked by the hooking thread's retry (it retries with the old parent).
+__device__ __forceinline__ uint32_t uf_find(uint32_t* L, uint32_t x) {
+  for (;;) {
+    const uint32_t p = L[x];
+    if (p == x) return x;
+    const uint32_t gp = L[p];
+    if (gp == p) return p;
+    L[x] = gp;
+    x = gp;
+  }
+}
+__device__ __forceinline__ void uf_union(uint32_t* L, uint32_t a, uint32_t b) {
+  // each retry follows a strictly smaller label, so this ends within n steps
+  for (uint32_t it = 0; it < 0x7fffffffu; ++it) {
+    a = uf_find(L, a);
+    b = uf_find(L, b);
+    if (a == b) return;
+    if (a < b) {
+      const uint32_t old = atomicMin(&L[b], a);
+      if (old == b) return;
+      b = old;
+    } else {
+      const uint32_t old = atomicMin(&L[a], b);
+      if (old == a) return;
+      a = old;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  uint32_t t = 0;
+  for (uint32_t k = 0; k < nw; ++k) t += red[k];
+  __syncthreads();
+  return t;
+}
+
+// Houdayer move (src/pt.rs:31-77) for the slots of `gmask` (bits of word w)
+// of chain pair (c0, c1) at sweep i: count the q<0 sites of every slot, draw
+// the seed index from Philox, label the q<0 subgraph by union-find, take the
+// seed's component, accumulate the energy change of flipping it in both
+// replicas (boundary terms, fixed point), and flip.  The result depends only
+// on the replica state, the seed and the sweep index -- not on the number of
+// threads or how slots are grouped -- so the fused and plain forms agree.
+__device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScratch& X, uint32_t i, uint32_t p,
+                          uint32_t w, uint32_t gmask) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  const uint32_t n = J.n;
+  const uint32_t n = J.n, T = blockDim.x;
+  const uint32_t o0 = 2 * p * J.wpc + w, o1 = (2 * p + 1) * J.wpc + w, tb = 32 * w;
+  for (uint32_t s = tid; s < n; s += T) {
+    X.D[s] = (W[s * J.nw + o0] ^ W[s * J.nw + o1]) & gmask;
+    X.Cl[s] = 0;
+  }
+  if (tid < 32) {
+    X.cnt[tid] = 0;
+    X.seed[tid] = 0xffffffffu;
+    X.gidx[tid] = __popc(gmask & ((1u << tid) - 1u));
+  }
+  if (tid < 64) X.dE[tid] = 0;
+  __syncthreads();
+  const uint32_t G = __popc(gmask);
+  if (G == 1) {
+    // one slot: block-wide count and ordered search for the k-th q<0 site
+    const uint32_t b = __ffs(gmask) - 1;
+    const uint32_t chunk = (n + T - 1) / T, s0 = min(n, tid * chunk), s1 = min(n, s0 + chunk);
+    uint32_t mine = 0;
+    for (uint32_t s = s0; s < s1; ++s) mine += (X.D[s] >> b) & 1u;
+    const uint32_t cnt = block_sum(mine, X.red);
+    if (cnt) {
+      const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;
+      const uint32_t k = (uint32_t)(((uint64_t)u * cnt) >> 32);
+      // exclusive prefix of the per-thread counts
+      uint32_t incl = mine;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+      }
+      if (lane == 31) X.red[warp] = incl;
+      __syncthreads();
+      uint32_t before = incl - mine;
+      for (uint32_t k2 = 0; k2 < warp; ++k2) before += X.red[k2];
+      if (k >= before && k < before + mine) {
+        uint32_t r = k - before;
+        for (uint32_t s = s0; s < s1; ++s)
+          if ((X.D[s] >> b) & 1u) {
+            if (r == 0) { X.seed[b] = s; break; }
+            --r;
+          }
+      }
+      if (tid == 0) X.cnt[b] = cnt;
+    }
+  } else {
+    // several slots: one warp per slot, ballot scans in site order
+    for (uint32_t b = warp; b < 32; b += nwarp) {
+      if (!((gmask >> b) & 1u)) continue;
+      uint32_t cnt = 0;
+      for (uint32_t base = 0; base < n; base += 32) {
+        const uint32_t s = base + lane;
+        cnt += __popc(__ballot_sync(0xffffffffu, s < n && ((X.D[s] >> b) & 1u)));
+      }
+      if (cnt == 0) continue;
+      const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;
+      uint32_t k = (uint32_t)(((uint64_t)u * cnt) >> 32);
+      for (uint32_t base = 0; base < n; base += 32) {
+        const uint32_t s = base + lane;
+        const uint32_t bal = __ballot_sync(0xffffffffu, s < n && ((X.D[s] >> b) & 1u));
+        const uint32_t c = __popc(bal);
+        if (k < c) {
+          if (lane == 0) {
+            X.seed[b] = base + __fns(bal, 0, (int)k + 1);
+            X.cnt[b] = cnt;
+          }
+          break;
+        }
+        k -= c;
+      }
+    }
+  }
+  __syncthreads();
+  // union-find labelling of the q<0 subgraph of every slot of the group, in
+  // four passes that keep the trees shallow:
+  //  (1) every site starts as a child of its smallest lower-index neighbour in
+  //      the subgraph, or as its own root;
+  //  (2) pointer jumping (find with path halving, then a store of the root):
+  //      every tree becomes a star;
+  //  (3) hooking: each subgraph edge whose ends have different roots links the
+  //      larger root under the smaller one (atomicMin, retried);
+  //  (4) pointer jumping again: every label is its component's root, the
+  //      smallest site index of the component.
+  for (uint32_t x = tid; x < G * n; x += T) X.L[x] = x % n;
+  __syncthreads();
+  for (uint32_t s = tid; s < n; s += T) {
+    const uint32_t d = X.D[s];
+    if (!d) continue;
+    const uint32_t e1 = F.rp[s + 1];
+    for (uint32_t e = F.rp[s]; e < e1; ++e) {
+      const uint32_t j = F.ent[e].x;
+      if (j >= s) continue;  // only this thread writes row s of every label array
+      uint32_t m = d & X.D[j];
+      while (m) {
+        const uint32_t b = __ffs(m) - 1;
+        m &= m - 1;
+        uint32_t* l = X.L + X.gidx[b] * n + s;
+        if (j < *l) *l = j;
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t g = 0; g < G; ++g)
+    for (uint32_t s = tid; s < n; s += T) X.L[g * n + s] = uf_find(X.L + g * n, s);
+  __syncthreads();
+  for (uint32_t s = tid; s < n; s += T) {
+    const uint32_t d = X.D[s];
+    if (!d) continue;
+    const uint32_t e1 = F.rp[s + 1];
+    for (uint32_t e = F.rp[s]; e < e1; ++e) {
+      const uint32_t j = F.ent[e].x;
+      if (j <= s) continue;  // every undirected edge once; self-loops skipped
+      uint32_t m = d & X.D[j];
+      while (m) {
+        const uint32_t b = __ffs(m) - 1;
+        m &= m - 1;
+        uint32_t* L = X.L + X.gidx[b] * n;
+        if (L[s] != L[j]) uf_union(L, s, j);
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t g = 0; g < G; ++g)
+    for (uint32_t s = tid; s < n; s += T) X.L[g * n + s] = uf_find(X.L + g * n, s);
+  __syncthreads();
+  // root of every seed, then the cluster: q<0 sites in the seed's component
+  if (tid < 32 && ((gmask >> tid) & 1u) && X.cnt[tid]) X.seed[tid] = X.L[X.gidx[tid] * n + X.seed[tid]];
+  __syncthreads();
+  for (uint32_t s = tid; s < n; s += T) {
+    uint32_t d = X.D[s], c = 0;
+    while (d) {
+      const uint32_t b = __ffs(d) - 1;
+      d &= d - 1;
+      if (X.cnt[b] && X.L[X.gidx[b] * n + s] == X.seed[b]) c |= 1u << b;
+    }
+    X.Cl[s] = c;
+  }
+  __syncthreads();
+  // energy change of flipping each cluster in both replicas: boundary terms
+  // -2 s_i (h_i + sum_{j not in cluster} J_ij s_j), f32 per site, summed in
+  // fixed point per slot: each warp reduces by shuffles, warps combine in a
+  // fixed order (no shared-memory 64-bit atomics)
+  for (uint32_t gm = gmask; gm;) {
+    const uint32_t b = __ffs(gm) - 1;
+    gm &= gm - 1;
+    long long a0 = 0, a1 = 0;
+    if (X.cnt[b]) {
+      for (uint32_t s = tid; s < n; s += T) {
+        if (!((X.Cl[s] >> b) & 1u)) continue;
+        const float h = F.bias[s];
+        float f0 = h, f1 = h;
+        const uint32_t e1 = F.rp[s + 1];
+        for (uint32_t e = F.rp[s]; e < e1; ++e) {
+          const uint2 ce = F.ent[e];
+          if (ce.x == s || ((X.Cl[ce.x] >> b) & 1u)) continue;
+          const float Jv = __uint_as_float(ce.y);
+          f0 += ((W[ce.x * J.nw + o0] >> b) & 1u) ? -Jv : Jv;
+          f1 += ((W[ce.x * J.nw + o1] >> b) & 1u) ? -Jv : Jv;
+        }
+        const float s0 = ((W[s * J.nw + o0] >> b) & 1u) ? -1.0f : 1.0f;
+        const float s1 = ((W[s * J.nw + o1] >> b) & 1u) ? -1.0f : 1.0f;
+        a0 += to_fx(-2.0f * s0 * f0);
+        a1 += to_fx(-2.0f * s1 * f1);
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+    }
+    if (lane == 0) {
+      X.part[warp * 2] = a0;
+      X.part[warp * 2 + 1] = a1;
+    }
+    __syncthreads();
+    if (tid < 2) {
+      long long t = 0;
+      for (uint32_t k = 0; k < nwarp; ++k) t += X.part[k * 2 + tid];
+      X.dE[tid * 32 + b] = (unsigned long long)t;
+    }
+    __syncthreads();
+  }
+  for (uint32_t s = tid; s < n; s += T) {
+    const uint32_t c = X.Cl[s];
+    if (c) {
+      atomicXor(&W[s * J.nw + o0], c);
+      atomicXor(&W[s * J.nw + o1], c);
+    }
+  }
+}
+
+// ICM phase of the fused kernel: all chain pairs, all slots >= lo, in groups
+// of at most J.icm_group slots (the label arrays that fit in shared memory).
+__device__ void icm_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i, PhaseClock& pc) {
+  const uint32_t tid = threadIdx.x;
   for (uint32_t p = 0; 2 * p + 1 < J.C; ++p) {
     const uint32_t c0 = 2 * p, c1 = 2 * p + 1;
     for (uint32_t w = 0; w < J.wpc; ++w) {
@@ -152,111 +452,28 @@ __device__ void icm_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i
       uint32_t lomask = 0;
       for (uint32_t b = 0; b < 32; ++b)
         if (tb + b >= J.lo && tb + b < J.nt) lomask |= 1u << b;
-      if (!lomask) continue;
-      const uint32_t o0 = c0 * J.wpc + w, o1 = c1 * J.wpc + w;
-      for (uint32_t s = tid; s < n; s += blockDim.x) {
-        S.D[s] = (S.W[s * J.nw + o0] ^ S.W[s * J.nw + o1]) & lomask;
-        S.Cl[s] = 0;
+      while (lomask) {
+        // next group: the lowest `icm_group` set bits
+        uint32_t gmask = 0, m = lomask;
+        for (uint32_t g = 0; g < J.icm_group && m; ++g) {
+          gmask |= m & (~m + 1u);
+          m &= m - 1;
+        }
+        lomask &= ~gmask;
+        icm_group(J, F, S.W, S.X, i, p, w, gmask);
+        __syncthreads();
+        pc.lap(PHASE_ICM_GROW);
+        if (tid < 32 && ((gmask >> tid) & 1u) && S.X.cnt[tid]) {
+          // the reference invalidates both caches; the next energy() is energy_ref
+          const uint32_t x0 = c0 * J.ntp + tb + tid, x1 = c1 * J.ntp + tb + tid;
+          S.Er[x0] += (double)(long long)S.X.dE[tid] * TAMC_FX_INV;
+          S.Er[x1] += (double)(long long)S.X.dE[32 + tid] * TAMC_FX_INV;
+          S.Ec[x0] = S.Er[x0];
+          S.Ec[x1] = S.Er[x1];
+        }
+        __syncthreads();
+        pc.lap(PHASE_ICM_APPLY);
       }
-      if (tid < 32) S.nneg[tid] = 0;
-      __syncthreads();
-      // count the q<0 sites per slot, draw the seed index, locate the seed
-      for (uint32_t b = warp; b < 32; b += nwarp) {
-        if (!((lomask >> b) & 1u)) continue;
-        uint32_t cnt = 0;
-        for (uint32_t base = 0; base < n; base += 32) {
-          const uint32_t s = base + lane;
-          cnt += __popc(__ballot_sync(0xffffffffu, s < n && ((S.D[s] >> b) & 1u)));
-        }
-        if (cnt == 0) continue;
-        const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;
-        uint32_t k = (uint32_t)(((uint64_t)u * cnt) >> 32);
-        for (uint32_t base = 0; base < n; base += 32) {
-          const uint32_t s = base + lane;
-          const uint32_t bal = __ballot_sync(0xffffffffu, s < n && ((S.D[s] >> b) & 1u));
-          const uint32_t c = __popc(bal);
-          if (k < c) {
-            const uint32_t pos = __fns(bal, 0, (int)k + 1);
-            if (lane == 0) {
-              atomicOr(&S.Cl[base + pos], 1u << b);
-              S.nneg[b] = cnt;
-            }
-            break;
-          }
-          k -= c;
-        }
-      }
-      __syncthreads();
-      // grow all clusters of this word to their fixed point
-      for (;;) {
-        int changed = 0;
-        for (uint32_t s = tid; s < n; s += blockDim.x) {
-          const uint32_t d = S.D[s];
-          if (!d) continue;
-          const uint32_t c = S.Cl[s];
-          const uint32_t rem = d & ~c;
-          if (!rem) continue;
-          uint32_t nb = 0;
-          const uint32_t e1 = F.rp[s + 1];
-          for (uint32_t e = F.rp[s]; e < e1; ++e) {
-            const uint32_t j = F.ent[e].x;
-            if (j != s) nb |= S.Cl[j];
-          }
-          const uint32_t add = rem & nb;
-          if (add) {
-            S.Cl[s] = c | add;
-            changed = 1;
-          }
-        }
-        if (!__syncthreads_or(changed)) break;
-      }
-      // energy change of flipping each cluster in both replicas (true Hamiltonian)
-      for (uint32_t b = warp; b < 32; b += nwarp) {
-        if (!S.nneg[b]) continue;
-        double a0 = 0, a1 = 0;
-        for (uint32_t s = lane; s < n; s += 32) {
-          if (!((S.Cl[s] >> b) & 1u)) continue;
-          const float h = F.bias[s];
-          float f0 = h, f1 = h;
-          const uint32_t e1 = F.rp[s + 1];
-          for (uint32_t e = F.rp[s]; e < e1; ++e) {
-            const uint2 ce = F.ent[e];
-            if (ce.x == s || ((S.Cl[ce.x] >> b) & 1u)) continue;
-            const float Jv = __uint_as_float(ce.y);
-            f0 += ((S.W[ce.x * J.nw + o0] >> b) & 1u) ? -Jv : Jv;
-            f1 += ((S.W[ce.x * J.nw + o1] >> b) & 1u) ? -Jv : Jv;
-          }
-          const float s0 = ((S.W[s * J.nw + o0] >> b) & 1u) ? -1.0f : 1.0f;
-          const float s1 = ((S.W[s * J.nw + o1] >> b) & 1u) ? -1.0f : 1.0f;
-          a0 += (double)(-2.0f * s0 * f0);
-          a1 += (double)(-2.0f * s1 * f1);
-        }
-        for (int off = 16; off > 0; off >>= 1) {
-          a0 += __shfl_xor_sync(0xffffffffu, a0, off);
-          a1 += __shfl_xor_sync(0xffffffffu, a1, off);
-        }
-        if (lane == 0) {
-          S.dE0[b] = a0;
-          S.dE1[b] = a1;
-        }
-      }
-      __syncthreads();
-      for (uint32_t s = tid; s < n; s += blockDim.x) {
-        const uint32_t c = S.Cl[s];
-        if (c) {
-          S.W[s * J.nw + o0] ^= c;
-          S.W[s * J.nw + o1] ^= c;
-        }
-      }
-      if (tid < 32 && S.nneg[tid]) {
-        // the reference invalidates both caches; the next energy() is energy_ref
-        const uint32_t x0 = c0 * J.ntp + tb + tid, x1 = c1 * J.ntp + tb + tid;
-        S.Er[x0] += S.dE0[tid];
-        S.Er[x1] += S.dE1[tid];
-        S.Ec[x0] = S.Er[x0];
-        S.Ec[x1] = S.Er[x1];
-      }
-      __syncthreads();
     }
   }
 }
@@ -441,33 +658,37 @@ __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32
   __shared__ uint32_t s_k, s_c, s_t;
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
   const uint32_t n = J.n, nt = J.nt, C = J.C;
-  // ground-state tracking (first minimum over slots, then chains; strict improvement)
-  if (tid == 0) {
-    float best = 0.0f;
-    uint32_t bc = 0, bt = 0;
-    for (uint32_t c = 0; c < C; ++c) {
-      uint32_t i1 = 0;
-      float e1 = (float)S.Ec[c * J.ntp];
-      for (uint32_t t = 1; t < nt; ++t) {
-        const float e = (float)S.Ec[c * J.ntp + t];
-        if (e < e1) { e1 = e; i1 = t; }
-      }
-      if (c == 0 || e1 < best) { best = e1; bc = c; bt = i1; }
+  // ground-state tracking: the reference takes the first minimum over slots,
+  // then the first over chains (lexicographic (E, chain, slot)), and records
+  // it when strictly below the running minimum.  Warp 0 reduces.
+  if (warp == 0) {
+    float be = INFINITY;
+    uint32_t bx = 0xffffffffu;
+    for (uint32_t x = lane; x < C * nt; x += 32) {
+      const float e = (float)S.Ec[(x / nt) * J.ntp + (x % nt)];
+      if (e < be || (e == be && x < bx)) { be = e; bx = x; }
     }
-    s_new = 0;
-    if (!*J.log.have || best < *J.log.minE) {
-      *J.log.have = 1;
-      *J.log.minE = best;
-      const uint32_t k = *J.log.count;
-      if (k < J.log.cap) {
-        J.log.steps[k] = i;
-        J.log.E[k] = best;
-        s_new = 1;
-        s_k = k;
-        s_c = bc;
-        s_t = bt;
+    for (int off = 16; off > 0; off >>= 1) {
+      const float oe = __shfl_xor_sync(0xffffffffu, be, off);
+      const uint32_t ox = __shfl_xor_sync(0xffffffffu, bx, off);
+      if (oe < be || (oe == be && ox < bx)) { be = oe; bx = ox; }
+    }
+    if (lane == 0) {
+      s_new = 0;
+      if (!*J.log.have || be < *J.log.minE) {
+        *J.log.have = 1;
+        *J.log.minE = be;
+        const uint32_t k = *J.log.count;
+        if (k < J.log.cap) {
+          J.log.steps[k] = i;
+          J.log.E[k] = be;
+          s_new = 1;
+          s_k = k;
+          s_c = bx / nt;
+          s_t = bx % nt;
+        }
+        *J.log.count = k + 1;
       }
-      *J.log.count = k + 1;
     }
   }
   __syncthreads();
@@ -529,7 +750,7 @@ __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32
 template <bool SELF>
 __device__ void run_job(const PtJob& J, char* smem_base) {
   Smem S;
-  carve_all(&S, smem_base, J.n, J.nw, J.C, J.ntp, J.qps, blockDim.x, J.F.nnz, J.csr_smem != 0);
+  carve_all(&S, smem_base, J.n, J.nw, J.C, J.ntp, J.qps, blockDim.x, J.F.nnz, J.csr_smem != 0, J.icm_group);
   const uint32_t tid = threadIdx.x, T = blockDim.x;
   const uint32_t n = J.n;
   FastInst F = J.F;
@@ -573,11 +794,16 @@ __device__ void run_job(const PtJob& J, char* smem_base) {
     if (J.init == 2) full_energies(J, F, S, Teff);
   }
   uint32_t m_cur = J.m_base, s_cur = J.s_base;
+  PhaseClock pc;
+  pc.start(J.prof);
   for (uint32_t i = J.sweep_begin; i < J.sweep_end; ++i) {
-    if (J.icm) icm_phase(J, F, S, i);
+    if (J.icm) icm_phase(J, F, S, i, pc);
     exchange_phase(J, S, i);
+    pc.lap(PHASE_EXCH);
     sweep_phase<SELF>(J, F, S, i, Teff);
+    pc.lap(PHASE_SWEEP);
     if (i >= J.meas_init) measure_phase(J, F, S, i, m_cur, s_cur);
+    pc.lap(PHASE_MEASURE);
   }
   for (uint32_t x = tid; x < n * J.nw; x += T) J.W[x] = S.W[x];
   for (uint32_t x = tid; x < J.C * J.ntp; x += T) {
@@ -615,10 +841,12 @@ __global__ void __launch_bounds__(512, 1) k_pt_fused(const PtJob* __restrict__ j
 // Markov chain bit for bit; the round index and measurement counters live in
 // device memory (PlainCtl) so a captured chunk of rounds replays unchanged.
 __host__ __device__ inline size_t plain_head_smem(uint32_t n, uint32_t C, uint32_t ntp) {
-  return al16((size_t)n * 4) * 2 + al16((size_t)C * ntp * 8) * 2 + al16(32 * 4) + al16(32 * 8) * 2 +
-         al16((size_t)C * 8);
+  (void)n;
+  return al16((size_t)C * ntp * 8) * 2 + al16((size_t)C * 8) + 64;
 }
 
+// Close the previous round (add its fixed-point sweep sums, measurements), or
+// (mode 2) set the initial energies from the energy kernel's sums.
 __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict__ jp, PlainCtl* ctl,
                                                        long long* acc, int mode) {
   extern __shared__ uint4 smem_u4[];
@@ -626,31 +854,20 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
   const uint32_t tid = threadIdx.x;
   char* base = reinterpret_cast<char*>(smem_u4);
   Smem S{};
-  size_t o = 0;
-  auto take = [&](size_t bytes) {
-    char* p = base + o;
-    o = al16(o + bytes);
-    return p;
-  };
-  S.D = (uint32_t*)take((size_t)J.n * 4);
-  S.Cl = (uint32_t*)take((size_t)J.n * 4);
-  S.Ec = (double*)take((size_t)J.C * J.ntp * 8);
-  S.Er = (double*)take((size_t)J.C * J.ntp * 8);
-  S.nneg = (uint32_t*)take(32 * 4);
-  S.dE0 = (double*)take(32 * 8);
-  S.dE1 = (double*)take(32 * 8);
-  S.Dm = (unsigned long long*)take((size_t)J.C * 8);
+  S.Ec = (double*)base;
+  S.Er = (double*)(base + al16((size_t)J.C * J.ntp * 8));
   S.W = J.W;
   const FastInst F = J.F;
   const uint32_t CN = J.C * J.ntp;
   long long* accq = acc + CN;
+  const bool pending = mode != 2 && ctl->pending;
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
     double ec = J.Ec[x], er = J.Er[x];
-    if (mode == 2) {  // initial energies from the fixed-point sums of the energy kernel
+    if (mode == 2) {
       ec = (double)J.F.offset + (double)acc[x] * TAMC_FX_INV;
       er = ec;
       acc[x] = 0;
-    } else if (ctl->pending) {  // IsingSampler::sweep: energy += Σ accepted ΔE
+    } else if (pending) {  // IsingSampler::sweep: energy += sum of accepted dE
       ec += (double)acc[x] * TAMC_FX_INV;
       er += (double)(acc[x] + accq[x]) * TAMC_FX_INV;
       acc[x] = 0;
@@ -661,44 +878,99 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
   }
   __syncthreads();
   uint32_t m_cur = ctl->m_cur, s_cur = ctl->s_cur;
-  if (mode != 2 && ctl->pending) {
+  PhaseClock pc;
+  pc.start(J.prof);
+  if (pending) {
     const uint32_t ip = ctl->i - 1;
     if (ip >= J.meas_init) measure_phase(J, F, S, ip, m_cur, s_cur);
-  }
-  __syncthreads();
-  if (mode == 0) {  // start round i: ICM, then exchange; the sweeps follow
-    const uint32_t i = ctl->i;
-    if (J.icm) icm_phase(J, F, S, i);
-    exchange_phase(J, S, i);
   }
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
     J.Ec[x] = S.Ec[x];
     J.Er[x] = S.Er[x];
   }
   __syncthreads();
+  pc.lap(PHASE_MEASURE);
   if (tid == 0) {
     ctl->m_cur = m_cur;
     ctl->s_cur = s_cur;
-    if (mode == 0) {
-      ctl->i += 1;
-      ctl->pending = 1;
-    } else {
-      ctl->pending = 0;
-    }
+    ctl->pending = 0;
     if (J.count_out) *J.count_out = *J.log.count;
   }
 }
 
+// Houdayer moves of round ctl->i: one CTA per (chain pair, slot >= lo).
+__global__ void __launch_bounds__(512) k_plain_icm(const PtJob* __restrict__ jp, const PlainCtl* __restrict__ ctl,
+                                                    long long* icm_dE, uint32_t* icm_valid) {
+  extern __shared__ uint4 smem_u4[];
+  const PtJob& J = *jp;
+  const uint32_t nact = J.nt - J.lo;
+  const uint32_t p = blockIdx.x / nact, t = J.lo + blockIdx.x % nact;
+  IcmScratch X;
+  carve_icm(&X, reinterpret_cast<char*>(smem_u4), 0, J.n, 1);
+  const uint32_t b = t & 31u;
+  icm_group(J, J.F, J.W, X, ctl->i, p, t >> 5, 1u << b);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t x0 = 2 * p * J.ntp + t, x1 = (2 * p + 1) * J.ntp + t;
+    const uint32_t v = X.cnt[b] != 0;
+    icm_valid[x0] = v;
+    icm_valid[x1] = v;
+    icm_dE[x0] = (long long)X.dE[b];
+    icm_dE[x1] = (long long)X.dE[32 + b];
+  }
+}
+
+// Energies after the Houdayer moves, replica exchange and the spin permutation
+// of round ctl->i; then the sweeps of that round may run.
+__global__ void __launch_bounds__(1024, 1) k_plain_exch(const PtJob* __restrict__ jp, PlainCtl* ctl,
+                                                       const long long* icm_dE, uint32_t* icm_valid) {
+  extern __shared__ uint4 smem_u4[];
+  const PtJob J = *jp;
+  const uint32_t tid = threadIdx.x;
+  char* base = reinterpret_cast<char*>(smem_u4);
+  Smem S{};
+  S.Ec = (double*)base;
+  S.Er = (double*)(base + al16((size_t)J.C * J.ntp * 8));
+  S.Dm = (unsigned long long*)(base + 2 * al16((size_t)J.C * J.ntp * 8));
+  S.W = J.W;
+  const uint32_t CN = J.C * J.ntp;
+  for (uint32_t x = tid; x < CN; x += blockDim.x) {
+    double ec = J.Ec[x], er = J.Er[x];
+    if (J.icm && icm_valid[x]) {  // invalidated caches are recomputed as energy_ref
+      er += (double)icm_dE[x] * TAMC_FX_INV;
+      ec = er;
+      icm_valid[x] = 0;
+    }
+    S.Ec[x] = ec;
+    S.Er[x] = er;
+  }
+  __syncthreads();
+  PhaseClock pc;
+  pc.start(J.prof);
+  const uint32_t i = ctl->i;
+  exchange_phase(J, S, i);
+  for (uint32_t x = tid; x < CN; x += blockDim.x) {
+    J.Ec[x] = S.Ec[x];
+    J.Er[x] = S.Er[x];
+  }
+  __syncthreads();
+  pc.lap(PHASE_EXCH);
+  if (tid == 0) {
+    ctl->i = i + 1;
+    ctl->pending = 1;
+  }
+}
+
+// The grid stride is a multiple of qps, so every thread keeps one quad k for
+// all its tasks and accumulates its fixed-point ΔE sums in registers; a CTA
+// combines its threads per slot and adds one 64-bit atomic per slot.
 template <bool SELF>
 __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ jp, const PlainCtl* __restrict__ ctl,
                                                      uint32_t color, long long* acc) {
   extern __shared__ uint4 smem_u4[];
   const PtJob& J = *jp;
-  const uint32_t CN = J.C * J.ntp;
-  long long* sacc = reinterpret_cast<long long*>(smem_u4);
-  long long* saccq = sacc + CN;
-  float4* b4 = reinterpret_cast<float4*>(saccq + CN + (CN & 1u));
-  for (uint32_t x = threadIdx.x; x < 2 * CN; x += blockDim.x) sacc[x] = 0;
+  Fx4* red = reinterpret_cast<Fx4*>(smem_u4);                 // [blockDim.x]
+  float4* b4 = reinterpret_cast<float4*>(red + blockDim.x);   // [qps]
   const float L2E = 1.4426950408889634f;
   for (uint32_t k = threadIdx.x; k < J.qps; k += blockDim.x) {
     const uint32_t q = k % J.qpc;
@@ -708,34 +980,47 @@ __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ j
   __syncthreads();
   const uint32_t i = ctl->i - 1;
   const uint32_t c0 = J.F.color_off[color], nc = J.F.color_off[color + 1] - c0;
-  const uint64_t ntask = (uint64_t)nc * J.qps;
+  const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t gstride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t k = (uint32_t)(gtid % J.qps);
+  const uint32_t ch = k / J.qpc, q = k % J.qpc;
+  const uint32_t wo = ch * J.wpc + (q >> 3), shift = 4 * (q & 7u);
+  const float4 bl2 = b4[k];
   const FastInst F = J.F;
-  for (uint64_t task = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; task < ntask;
-       task += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t k = (uint32_t)(task % J.qps);
-    const uint32_t s = c0 + (uint32_t)(task / J.qps);
-    const uint32_t ch = k / J.qpc, q = k % J.qpc;
-    const uint32_t wo = ch * J.wpc + (q >> 3), shift = 4 * (q & 7u);
+  Fx4 a{0, 0, 0, 0}, aq{0, 0, 0, 0};
+  for (uint64_t site = gtid / J.qps; site < nc; site += gstride / J.qps) {
+    const uint32_t s = c0 + (uint32_t)site;
     const uint4 rnd = philox4x32_10(make_uint4(s, i, ch * 16u + q, PTAG_SWEEP), J.key);
-    Fx4 a{0, 0, 0, 0};
-    const uint32_t m = quad_update<true>(s, shift, F, J.W, J.nw, wo, b4[k], rnd, a);
+    const uint32_t m = quad_update<true>(s, shift, F, J.W, J.nw, wo, bl2, rnd, a);
     if (m) {
       atomicXor(&J.W[s * J.nw + wo], m << shift);
-      const uint32_t slot = ch * J.ntp + 4 * q;
-      if (m & 1u) atomicAdd((unsigned long long*)&sacc[slot + 0], (unsigned long long)a.x);
-      if (m & 2u) atomicAdd((unsigned long long*)&sacc[slot + 1], (unsigned long long)a.y);
-      if (m & 4u) atomicAdd((unsigned long long*)&sacc[slot + 2], (unsigned long long)a.z);
-      if (m & 8u) atomicAdd((unsigned long long*)&sacc[slot + 3], (unsigned long long)a.w);
       if (SELF) {
-        const unsigned long long k2 = (unsigned long long)to_fx(2.0f * F.kd[s]);
-        for (uint32_t r = 0; r < 4; ++r)
-          if ((m >> r) & 1u) atomicAdd((unsigned long long*)&saccq[slot + r], k2);
+        const long long k2 = to_fx(2.0f * F.kd[s]);
+        aq.x += (m & 1u) ? k2 : 0;
+        aq.y += (m & 2u) ? k2 : 0;
+        aq.z += (m & 4u) ? k2 : 0;
+        aq.w += (m & 8u) ? k2 : 0;
       }
     }
   }
-  __syncthreads();
-  for (uint32_t x = threadIdx.x; x < 2 * CN; x += blockDim.x)
-    if (sacc[x]) atomicAdd((unsigned long long*)&acc[x], (unsigned long long)sacc[x]);
+  const uint32_t CN = J.C * J.ntp;
+  for (int pass = 0; pass < (SELF ? 2 : 1); ++pass) {
+    red[threadIdx.x] = pass ? aq : a;
+    __syncthreads();
+    // threads of this CTA holding quad kk: tid with (blockIdx.x*blockDim.x + tid) % qps == kk
+    for (uint32_t x = threadIdx.x; x < CN; x += blockDim.x) {
+      const uint32_t c = x / J.ntp, t = x % J.ntp;
+      const uint32_t kk = c * J.qpc + t / 4;
+      const uint32_t first = (uint32_t)((kk + J.qps - (uint64_t)blockIdx.x * blockDim.x % J.qps) % J.qps);
+      long long sum = 0;
+      for (uint32_t th = first; th < blockDim.x; th += J.qps) {
+        const Fx4 v = red[th];
+        sum += (t & 3u) == 0 ? v.x : (t & 3u) == 1 ? v.y : (t & 3u) == 2 ? v.z : v.w;
+      }
+      if (sum) atomicAdd((unsigned long long*)&acc[pass * CN + x], (unsigned long long)sum);
+    }
+    __syncthreads();
+  }
 }
 
 // Initial replicas (random, as the fused kernel's init) and their energy terms.
@@ -777,7 +1062,7 @@ __global__ void k_plain_energy(const PtJob* __restrict__ jp, long long* acc) {
 }  // namespace
 
 size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem) {
-  return carve_all(nullptr, nullptr, j.n, j.nw, j.C, j.ntp, j.qps, T, j.F.nnz, csr_smem);
+  return carve_all(nullptr, nullptr, j.n, j.nw, j.C, j.ntp, j.qps, T, j.F.nnz, csr_smem, j.icm_group);
 }
 
 int fused_blocks_per_sm(uint32_t T, size_t smem) {
@@ -795,11 +1080,34 @@ void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long 
   TAMC_CUDA(cudaGetLastError());
 }
 
+size_t plain_icm_bytes(const PtJob& j) { return carve_icm(nullptr, nullptr, 0, j.n, 1); }
+
+void plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, long long* icm_dE,
+                      uint32_t* icm_valid) {
+  const uint32_t nact = j.nt - j.lo, grid = (j.C / 2) * nact;
+  if (!j.icm || grid == 0) return;
+  const size_t smem = plain_icm_bytes(j);
+  TAMC_CUDA(cudaFuncSetAttribute(k_plain_icm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_plain_icm<<<grid, 512, smem, st>>>(d_job, ctl, icm_dE, icm_valid);
+  TAMC_CUDA(cudaGetLastError());
+}
+
+void plain_launch_exch(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, const long long* icm_dE,
+                       uint32_t* icm_valid) {
+  const size_t smem = plain_head_smem(j.n, j.C, j.ntp);
+  TAMC_CUDA(cudaFuncSetAttribute(k_plain_exch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_plain_exch<<<1, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid);
+  TAMC_CUDA(cudaGetLastError());
+}
+
 void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, uint32_t color,
                         uint32_t ntask, long long* acc, uint32_t grid_cap) {
   const uint32_t T = 256;
-  const uint32_t grid = std::max(1u, std::min(grid_cap, (ntask + T - 1) / T));
-  const size_t smem = (size_t)(2 * j.C * j.ntp + 2) * 8 + (size_t)j.qps * 16;
+  uint32_t grid = std::max(1u, std::min(grid_cap, (ntask + T - 1) / T));
+  // grid * T must be a multiple of qps (each thread keeps one quad)
+  const uint32_t g = j.qps / std::gcd(j.qps, T);
+  grid = std::max(g, (grid + g - 1) / g * g);
+  const size_t smem = (size_t)T * sizeof(Fx4) + (size_t)j.qps * 16;
   if (j.self_loops) {
     TAMC_CUDA(cudaFuncSetAttribute(k_plain_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_plain_sweep<true><<<grid, T, smem, st>>>(d_job, ctl, color, acc);

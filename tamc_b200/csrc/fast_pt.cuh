@@ -14,6 +14,7 @@ struct PtJob {
   uint32_t n, nt, ntp, C, wpc, nw, lo, qpc, qps;
   int32_t icm, threaded, self_loops, csr_smem;
   int32_t init;        // 0: load state, 1: random spins + energies, 2: load spins + energies
+  uint32_t icm_group;  // ICM slots labelled together (label arrays in shared memory)
   const float* betas;  // [ntp], padding slots have beta = 0
   uint2 key;
   uint32_t* W;         // [n][nw]
@@ -29,8 +30,12 @@ struct PtJob {
   MeasOut out;
   GsLog log;
   uint32_t* count_out; // if set: receives the log count when the job's range is done
+  unsigned long long* prof;  // if set: per-phase clock64 cycles (PHASE_* order), off otherwise
   uint64_t cost;       // sweeps * n * R, for longest-first ordering
 };
+
+enum { PHASE_ICM_SCAN, PHASE_ICM_GROW, PHASE_ICM_APPLY, PHASE_EXCH, PHASE_SWEEP, PHASE_MEASURE, PHASE_OTHER,
+       PHASE_N };
 
 // Shared-memory bytes the fused kernel needs for a job with T threads.
 size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem);
@@ -48,8 +53,15 @@ struct PlainCtl {
   uint32_t pending;  // the sweeps of round i-1 ran; their sums and measurements are pending
 };
 size_t plain_head_bytes(const PtJob& j);
-// mode 0: close the previous round and start round ctl->i; 1: only close; 2: set initial energies
+// mode 1: close the previous round (sweep sums, measurements); 2: set initial energies
 void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem);
+size_t plain_icm_bytes(const PtJob& j);
+// Houdayer moves of round ctl->i, one CTA per (chain pair, slot >= lo)
+void plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, long long* icm_dE,
+                      uint32_t* icm_valid);
+// energies after ICM, exchange, spin permutation; advances ctl->i
+void plain_launch_exch(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, const long long* icm_dE,
+                       uint32_t* icm_valid);
 void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, uint32_t color,
                         uint32_t ntask, long long* acc, uint32_t grid_cap);
 void plain_launch_init(cudaStream_t st, const PtJob* d_job, long long* acc, int random, uint32_t grid);
@@ -61,6 +73,7 @@ void fast_pt_get_state(tamc_pt* pt, int8_t* spins, float* energies);
 void fast_pt_set_state(tamc_pt* pt, const int8_t* spins);
 void fast_pt_acceptance(tamc_pt* pt, uint32_t* acc);
 void fast_pt_round_trips(tamc_pt* pt, uint8_t* tags, uint32_t* round_trips, uint32_t* dhist);
+void fast_pt_phase_cycles(tamc_pt* pt, uint64_t* out);
 void fast_pt_destroy(tamc_pt* pt);
 
 }  // namespace tamc

@@ -11,6 +11,7 @@
 #include "fast_common.cuh"
 #include "fast_sa.cuh"
 
+#include <cstdio>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -59,13 +60,14 @@ __global__ void __launch_bounds__(1024) k_sa_fast(SaFastArgs a) {
   const uint32_t qid = (r0 >> 2) + q;
   const uint32_t stride = T / NQ;
   Fx4 acc{0, 0, 0, 0};  // unused: SA energies are computed once at the end
+  const PhiloxKeys PK = philox_schedule(key);
   for (uint32_t sw = 0; sw < a.nbeta; ++sw) {
     const float b = a.betas[sw] * 1.4426950408889634f;  // beta * log2(e)
     const float4 beta = make_float4(b, b, b, b);
     for (uint32_t c = 0; c < F.ncolors; ++c) {
       const uint32_t c1 = a.F.color_off[c + 1];
       for (uint32_t s = a.F.color_off[c] + tid / NQ; s < c1; s += stride) {
-        const uint4 rnd = philox4x32_10(make_uint4(s, sw, qid, PTAG_SWEEP), key);
+        const uint4 rnd = philox4x32_10(make_uint4(s, sw, qid, PTAG_SWEEP), PK);
         const uint32_t m = quad_update<false>(s, shift, F, W, 1, 0, beta, rnd, acc);
         if (m) {
           if (NQ == 1) W[s] ^= m;
@@ -240,14 +242,19 @@ SaTile sa_fast_choose(tamc_gpu* g, const FastInst& F, uint32_t R) {
     cudaFree(d_e);
     cudaFree(d_w);
   }
-  if (const char* e = getenv("TAMC_SA_NQ")) {
+  if (const char* e = getenv("TAMC_SA_NQ")) {  // manual override (profiling)
     const int v = atoi(e);
-    if (v == 1 || v == 2 || v == 4 || v == 8) {
-      best.nq = (uint32_t)v;
-      best.smem = sa_fast_smem(F, best.nq, best.T, best.smem_csr);
-    }
+    if (v == 1 || v == 2 || v == 4 || v == 8) best.nq = (uint32_t)v;
   }
+  if (const char* e = getenv("TAMC_SA_T")) {
+    const int v = atoi(e);
+    if (v == 256 || v == 512 || v == 1024) best.T = (uint32_t)v;
+  }
+  best.smem = sa_fast_smem(F, best.nq, best.T, best.smem_csr);
   if (best.smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the fast SA kernel");
+  if (getenv("TAMC_DEBUG"))
+    fprintf(stderr, "[tamc] SA tile n=%u R=%u: replicas/CTA=%u threads=%u csr_smem=%d smem=%zu\n", F.n, R,
+            4 * best.nq, best.T, (int)best.smem_csr, best.smem);
   std::lock_guard<std::mutex> lk(g_sa_mu);
   g_sa_tune[key] = best;
   return best;

@@ -430,6 +430,14 @@ int tamc_gpu_pt_samples(tamc_pt* pt, float* e, int32_t* q, float* suscept, uint8
   TAMC_API_END
 }
 
+int tamc_gpu_pt_phase_cycles(tamc_pt* pt, uint64_t* cycles) {
+  TAMC_API_BEGIN
+  if (!pt || !cycles) fail(TAMC_E_INVAL, "null argument");
+  if (pt->mode != TAMC_MODE_FAST) fail(TAMC_E_INVAL, "phase accounting exists in fast mode only");
+  fast_pt_phase_cycles(pt, cycles);
+  TAMC_API_END
+}
+
 double tamc_gpu_pt_timing_us(tamc_pt* pt) { return pt ? pt->timing_us : 0.0; }
 
 int tamc_gpu_pt_destroy(tamc_pt* pt) {
