@@ -174,8 +174,10 @@ int tamc_gpu_pt_samples_dims(tamc_pt* pt, uint32_t* M, uint32_t* S, uint32_t* Z,
  * any pointer may be NULL to skip it. */
 int tamc_gpu_pt_samples(tamc_pt* pt, float* e, int32_t* q, float* suscept, uint8_t* samples);
 /* Fast mode with TAMC_PHASE_PROF=1 in the environment at creation: SM cycles
- * spent per round phase (ICM scan, ICM cluster growth, ICM apply, exchange,
- * sweep, measurement, other), summed over rounds; zeros otherwise. cycles[7]. */
+ * spent per round phase (ICM: seed scan, union-find label init, pointer
+ * jumping, cluster growth (BFS levels or union-find hooking), cluster marking,
+ * energy change and flip; exchange, sweep, measurement, other), summed over
+ * rounds; zeros otherwise.  cycles[10]. */
 int tamc_gpu_pt_phase_cycles(tamc_pt* pt, uint64_t* cycles);
 /* Wall time of the sweep loop in microseconds (the reference's `timing`). */
 double tamc_gpu_pt_timing_us(tamc_pt* pt);

@@ -430,11 +430,12 @@ class PtRun:
     def timing_us(self) -> float:
         return lib().tamc_gpu_pt_timing_us(self.h)
 
-    PHASES = ("icm_scan", "icm_grow", "icm_apply", "exchange", "sweep", "measure", "other")
+    PHASES = ("icm_scan", "icm_init", "icm_jump", "icm_grow", "icm_mark", "icm_apply", "exchange", "sweep", "measure",
+              "other")
 
     def phase_cycles(self) -> dict:
         """Cycles per round phase (fast mode, TAMC_PHASE_PROF=1 at creation)."""
-        a = np.zeros(7, np.uint64)
+        a = np.zeros(len(self.PHASES), np.uint64)
         _check(lib().tamc_gpu_pt_phase_cycles(self.h, _p(a, u64p)))
         return dict(zip(self.PHASES, a.tolist()))
 

@@ -99,7 +99,9 @@ int tamc_gpu_open(int device, tamc_gpu** out) {
   auto* g = new tamc_gpu();
   g->device = device;
   g->num_sms = prop.multiProcessorCount;
-  g->smem_optin = prop.sharedMemPerBlockOptin;
+  // dynamic shared memory a launch may ask for: the opt-in limit less 1 KB for
+  // the kernels' static shared memory (job descriptor copies, counters)
+  g->smem_optin = prop.sharedMemPerBlockOptin - 1024;
   try {
     TAMC_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     const size_t blob = (size_t)(tamc_expf_blob_end - tamc_expf_blob_begin);

@@ -52,7 +52,7 @@ struct TileChoice {
   bool csr;
 };
 static std::mutex g_tune_mu;
-static std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t, int>, TileChoice> g_tune;
+static std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t, int, int>, TileChoice> g_tune;
 
 static bool fits(const tamc_gpu* g, const PtJob& j, uint32_t T, bool csr) {
   return fused_smem_bytes(j, T, csr) <= g->smem_optin;
@@ -117,7 +117,7 @@ thread_local bool g_no_autotune = false;
 
 static TileChoice tune_tile(tamc_gpu* g, const PtJob& j) {
   if (g_no_autotune) return heuristic_tile(g, j);
-  const auto key = std::make_tuple(g->device, j.n, j.F.nnz, j.nt, j.C, (int)j.self_loops);
+  const auto key = std::make_tuple(g->device, j.n, j.F.nnz, j.nt, j.C, (int)j.self_loops, (int)j.icm_uf);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
@@ -224,6 +224,10 @@ static void fill_job(tamc_pt* pt, uint64_t seed, tamc_pt::FastState* F) {
     for (uint32_t b = 0; b < 32; ++b) a += (32 * w + b >= j.lo && 32 * w + b < j.nt);
     active = std::max(active, a);
   }
+  // cluster search: frontier BFS unless TAMC_ICM=uf asks for union-find
+  // labelling (same clusters; BFS touches only the clusters)
+  j.icm_uf = 0;
+  if (const char* e = getenv("TAMC_ICM")) j.icm_uf = strcmp(e, "uf") == 0;
   const size_t budget = std::min<size_t>(pt->g->smem_optin, 110 * 1024);
   j.icm_group = std::max(1u, active);
   while (j.icm_group > 1 && fused_smem_bytes(j, 512, false) > budget) --j.icm_group;
@@ -261,7 +265,7 @@ static void plain_enqueue_rounds(tamc_pt* pt, uint32_t K) {
   const auto& off = pt->inst->color_off;
   for (uint32_t r = 0; r < K; ++r) {
     plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem);
-    plain_launch_icm(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p);
+    plain_launch_icm(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, pt->g->smem_optin);
     plain_launch_exch(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p);
     for (uint32_t c = 0; c + 1 < off.size(); ++c)
       plain_launch_sweep(st, j, F->d_job.p, F->ctl.p, c, (off[c + 1] - off[c]) * j.qps, F->eacc.p, F->grid_cap);
@@ -321,7 +325,7 @@ static void plain_init_energies(tamc_pt* pt, bool random) {
 // Which form runs a single instance: the fused kernel (one CTA, state in
 // shared memory) or the plain form (all SMs, state in L2/HBM).  Both give the
 // same results; the autotuner times a few rounds of each on this shape.
-static std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t>, bool> g_form;
+static std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, uint32_t, int>, bool> g_form;
 
 static bool choose_plain(tamc_pt* pt) {
   const char* f = getenv("TAMC_PT_FORM");
@@ -332,7 +336,7 @@ static bool choose_plain(tamc_pt* pt) {
   const bool fused_fits = fused_smem_bytes(j, 128, false) <= pt->g->smem_optin;
   const bool plain_fits = plain_head_bytes(j) <= pt->g->smem_optin;
   if (!fused_fits || !plain_fits) return !fused_fits;
-  const auto key = std::make_tuple(pt->g->device, j.n, j.F.nnz, j.nt, j.C);
+  const auto key = std::make_tuple(pt->g->device, j.n, j.F.nnz, j.nt, j.C, (int)j.icm_uf);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_form.find(key);
@@ -532,12 +536,19 @@ struct ChunkRunner {
     };
     std::stable_sort(act.begin(), act.end(), [&](tamc_pt* x, tamc_pt* y) { return remaining(x) > remaining(y); });
     // one CTA size per launch: the autotuned size of the costliest run
+    // (TAMC_PT_T and TAMC_PT_CSR=0 override it for measurements)
     uint32_t T = act[0]->fast->T;
+    if (const char* e = getenv("TAMC_PT_T")) {
+      const int t = atoi(e);
+      if (t == 128 || t == 256 || t == 512) T = (uint32_t)t;
+    }
+    const char* csr_env = getenv("TAMC_PT_CSR");
     for (auto* pt : act)
       if (T < pt->fast->job.qps) T = 512;
     size_t smem = 0;
     for (auto* pt : act) {
       PtJob& j = pt->fast->job;
+      if (csr_env && csr_env[0] == '0') j.csr_smem = 0;
       if (fused_smem_bytes(j, T, j.csr_smem) > g->smem_optin) j.csr_smem = 0;
       smem = std::max(smem, fused_smem_bytes(j, T, j.csr_smem));
     }

@@ -60,13 +60,14 @@ __device__ __forceinline__ float u24(uint32_t r) { return (float)(r >> 8) * (1.0
 struct IcmScratch {
   uint32_t* D;     // [n] disagreement bits of the group's slots
   uint32_t* Cl;    // [n] cluster bits
-  uint32_t* L;     // [G][n] union-find labels, G = popcount of the group mask
+  uint32_t* L;     // union-find: [G][n] labels; BFS: [4][n] two frontiers, visited list, level marks
   uint32_t* cnt;   // [32] q<0 counts per bit
   uint32_t* seed;  // [32] seed site per bit
   uint32_t* gidx;  // [32] label-array index per bit
   unsigned long long* dE;  // [2][32] fixed-point energy change per chain and bit
   uint32_t* red;   // [32] block reduction scratch
   long long* part; // [32 warps][2] per-warp partial sums
+  uint32_t* q;     // [4] BFS counters: frontier sizes (three, by level mod 3), visited count
 };
 
 struct Smem {
@@ -85,7 +86,12 @@ struct Smem {
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-__host__ __device__ inline size_t carve_icm(IcmScratch* X, char* base, size_t o, uint32_t n, uint32_t G) {
+// Label region: G label arrays for union-find, four site arrays for BFS.
+__host__ __device__ inline size_t icm_label_words(uint32_t n, uint32_t G, bool uf) {
+  return (size_t)(uf ? G : 4u) * n;
+}
+
+__host__ __device__ inline size_t carve_icm(IcmScratch* X, char* base, size_t o, uint32_t n, uint32_t G, bool uf) {
   auto take = [&](size_t bytes) {
     char* p = base ? base + o : nullptr;
     o = al16(o + bytes);
@@ -93,13 +99,14 @@ __host__ __device__ inline size_t carve_icm(IcmScratch* X, char* base, size_t o,
   };
   char* D = take((size_t)n * 4);
   char* Cl = take((size_t)n * 4);
-  char* L = take((size_t)G * n * 4);
+  char* L = take(icm_label_words(n, G, uf) * 4);
   char* cnt = take(32 * 4);
   char* seed = take(32 * 4);
   char* gidx = take(32 * 4);
   char* dE = take(64 * 8);
   char* red = take(32 * 4);
   char* part = take(64 * 8);
+  char* q = take(4 * 4);
   if (X) {
     X->D = (uint32_t*)D;
     X->Cl = (uint32_t*)Cl;
@@ -110,12 +117,14 @@ __host__ __device__ inline size_t carve_icm(IcmScratch* X, char* base, size_t o,
     X->dE = (unsigned long long*)dE;
     X->red = (uint32_t*)red;
     X->part = (long long*)part;
+    X->q = (uint32_t*)q;
   }
   return o;
 }
 
 __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uint32_t nw, uint32_t C, uint32_t ntp,
-                                            uint32_t qps, uint32_t T, uint32_t nnz, bool csr, uint32_t G) {
+                                            uint32_t qps, uint32_t T, uint32_t nnz, bool csr, uint32_t G,
+                                            bool uf) {
   size_t o = 0;
   auto take = [&](size_t bytes) {
     char* p = base ? base + o : nullptr;
@@ -124,7 +133,7 @@ __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uin
   };
   char* W = take((size_t)n * nw * 4);
   IcmScratch X;
-  o = carve_icm(&X, base, o, n, G);
+  o = carve_icm(&X, base, o, n, G, uf);
   char* Ec = take((size_t)C * ntp * 8);
   char* Er = take((size_t)C * ntp * 8);
   char* b4 = take((size_t)qps * 16);
@@ -193,42 +202,16 @@ __device__ void full_energies(const PtJob& J, const FastInst& F, Smem& S, uint32
 }
 
 // ------------------------------------------------------------------ ICM ----
-// Union-find connected-component labelling on the subgraph where the two
-// replicas of a slot disagree.  Labels are site indices; a root is its own
-// label and every label points to a smaller-or-equal index, so `uf_find`
-// terminates and concurrent hooking (atomicMin of the larger root onto the
-// smaller) is lock-free.
-// find with path halving: every visited node is re-pointed at its
-// grandparent.  A plain store is enough: the new parent is an ancestor of the
-// node, and a concurrent atomicMin hook that such a store overwrites is
-// re-linked by the hooking thread's retry (it retries with the old parent).
-__device__ __forceinline__ uint32_t uf_find(uint32_t* L, uint32_t x) {
-  for (;;) {
-    const uint32_t p = L[x];
-    if (p == x) return x;
-    const uint32_t gp = L[p];
-    if (gp == p) return p;
-    L[x] = gp;
-    x = gp;
-  }
-}
-__device__ __forceinline__ void uf_union(uint32_t* L, uint32_t a, uint32_t b) {
-  // each retry follows a strictly smaller label, so this ends within n steps
-  for (uint32_t it = 0; it < 0x7fffffffu; ++it) {
-    a = uf_find(L, a);
-    b = uf_find(L, b);
-    if (a == b) return;
-    if (a < b) {
-      const uint32_t old = atomicMin(&L[b], a);
-      if (old == b) return;
-      b = old;
-    } else {
-      const uint32_t old = atomicMin(&L[a], b);
-      if (old == a) return;
-      a = old;
-    }
-  }
-}
+// Connected components of the subgraph where the two replicas of a slot
+// disagree, by union-find in rounds (Shiloach-Vishkin style): labels are site
+// indices, every label points to a smaller-or-equal index (a root is its own
+// label), pointer jumping turns the trees into stars, and hooking links the
+// larger of two adjacent roots under the smaller with atomicMin.  A hook that
+// lands on a root another thread has already hooked in the same round may
+// drop that link; the edge still joins two labels afterwards and is hooked
+// again in the next round.  Every round removes at least one root, so the
+// rounds end within n + 1, and the final labels are the smallest site index
+// of each component whatever the thread schedule was.
 
 __device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -244,20 +227,45 @@ __device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red) {
 
 // Houdayer move (src/pt.rs:31-77) for the slots of `gmask` (bits of word w)
 // of chain pair (c0, c1) at sweep i: count the q<0 sites of every slot, draw
-// the seed index from Philox, label the q<0 subgraph by union-find, take the
-// seed's component, accumulate the energy change of flipping it in both
-// replicas (boundary terms, fixed point), and flip.  The result depends only
-// on the replica state, the seed and the sweep index -- not on the number of
-// threads or how slots are grouped -- so the fused and plain forms agree.
+// the seed index from Philox, find the seed's component of the q<0 subgraph,
+// accumulate the energy change of flipping it in both replicas (boundary
+// terms, fixed point), and flip.  The component is found either by a
+// level-synchronous BFS from the seeds of all slots at once (bit-parallel:
+// the cluster word of a site carries one bit per slot, and only cluster
+// sites and their edges are touched) or by union-find labelling of the whole
+// subgraph (J.icm_uf).  Both give the exact component, so the result depends
+// only on the replica state, the seed and the sweep index -- not on the
+// algorithm, the number of threads or how slots are grouped -- and the fused
+// and plain forms agree.
 __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScratch& X, uint32_t i, uint32_t p,
-                          uint32_t w, uint32_t gmask) {
+                          uint32_t w, uint32_t gmask, const uint16_t* cols = nullptr, uint32_t* wstage = nullptr,
+                          PhaseClock* pc = nullptr) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  const uint32_t n = J.n, T = blockDim.x;
+  const uint32_t n = J.n, T = blockDim.x, nw = J.nw;
   const uint32_t o0 = 2 * p * J.wpc + w, o1 = (2 * p + 1) * J.wpc + w, tb = 32 * w;
+  // loop-invariant pointers in registers (stores through the label arrays
+  // would otherwise force reloads of the descriptors)
+  const uint32_t* __restrict__ rp = F.rp;
+  const uint2* __restrict__ ent = F.ent;
+  const float* __restrict__ bias = F.bias;
+  uint32_t* const XD = X.D;
+  uint32_t* const XC = X.Cl;
+  uint32_t* const XL = X.L;
+  const bool uf = J.icm_uf != 0;
+  // the pair's replica words, read once (kept in shared memory when W is not)
+  auto r0 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[s] : W[s * nw + o0]; };
+  auto r1 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[n + s] : W[s * nw + o1]; };
   for (uint32_t s = tid; s < n; s += T) {
-    X.D[s] = (W[s * J.nw + o0] ^ W[s * J.nw + o1]) & gmask;
-    X.Cl[s] = 0;
+    const uint32_t v0 = W[s * nw + o0], v1 = W[s * nw + o1];
+    if (wstage) {
+      wstage[s] = v0;
+      wstage[n + s] = v1;
+    }
+    XD[s] = (v0 ^ v1) & gmask;
+    XC[s] = 0;
+    if (!uf) XL[3 * n + s] = 0;  // BFS level marks
   }
+  if (tid < 4) X.q[tid] = 0;
   if (tid < 32) {
     X.cnt[tid] = 0;
     X.seed[tid] = 0xffffffffu;
@@ -271,7 +279,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     const uint32_t b = __ffs(gmask) - 1;
     const uint32_t chunk = (n + T - 1) / T, s0 = min(n, tid * chunk), s1 = min(n, s0 + chunk);
     uint32_t mine = 0;
-    for (uint32_t s = s0; s < s1; ++s) mine += (X.D[s] >> b) & 1u;
+    for (uint32_t s = s0; s < s1; ++s) mine += (XD[s] >> b) & 1u;
     const uint32_t cnt = block_sum(mine, X.red);
     if (cnt) {
       const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;
@@ -289,7 +297,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
       if (k >= before && k < before + mine) {
         uint32_t r = k - before;
         for (uint32_t s = s0; s < s1; ++s)
-          if ((X.D[s] >> b) & 1u) {
+          if ((XD[s] >> b) & 1u) {
             if (r == 0) { X.seed[b] = s; break; }
             --r;
           }
@@ -303,14 +311,14 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
       uint32_t cnt = 0;
       for (uint32_t base = 0; base < n; base += 32) {
         const uint32_t s = base + lane;
-        cnt += __popc(__ballot_sync(0xffffffffu, s < n && ((X.D[s] >> b) & 1u)));
+        cnt += __popc(__ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u)));
       }
       if (cnt == 0) continue;
       const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;
       uint32_t k = (uint32_t)(((uint64_t)u * cnt) >> 32);
       for (uint32_t base = 0; base < n; base += 32) {
         const uint32_t s = base + lane;
-        const uint32_t bal = __ballot_sync(0xffffffffu, s < n && ((X.D[s] >> b) & 1u));
+        const uint32_t bal = __ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u));
         const uint32_t c = __popc(bal);
         if (k < c) {
           if (lane == 0) {
@@ -324,119 +332,224 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     }
   }
   __syncthreads();
-  // union-find labelling of the q<0 subgraph of every slot of the group, in
-  // four passes that keep the trees shallow:
-  //  (1) every site starts as a child of its smallest lower-index neighbour in
-  //      the subgraph, or as its own root;
-  //  (2) pointer jumping (find with path halving, then a store of the root):
-  //      every tree becomes a star;
-  //  (3) hooking: each subgraph edge whose ends have different roots links the
-  //      larger root under the smaller one (atomicMin, retried);
-  //  (4) pointer jumping again: every label is its component's root, the
-  //      smallest site index of the component.
-  for (uint32_t x = tid; x < G * n; x += T) X.L[x] = x % n;
-  __syncthreads();
-  for (uint32_t s = tid; s < n; s += T) {
-    const uint32_t d = X.D[s];
-    if (!d) continue;
-    const uint32_t e1 = F.rp[s + 1];
-    for (uint32_t e = F.rp[s]; e < e1; ++e) {
-      const uint32_t j = F.ent[e].x;
-      if (j >= s) continue;  // only this thread writes row s of every label array
-      uint32_t m = d & X.D[j];
-      while (m) {
-        const uint32_t b = __ffs(m) - 1;
-        m &= m - 1;
-        uint32_t* l = X.L + X.gidx[b] * n + s;
-        if (j < *l) *l = j;
+  if (pc) pc->lap(PHASE_ICM_SCAN);
+  auto col = [&](uint32_t e) -> uint32_t { return cols ? cols[e] : ent[e].x; };
+  const uint32_t* vlist = nullptr;  // BFS: the cluster sites; union-find: all sites
+  if (uf) {
+    // union-find labelling of the q<0 subgraph of every slot of the group:
+    // (1) every site starts as a child of its smallest lower-index neighbour in
+    //     the subgraph, or as its own root;
+    // (2) rounds of pointer jumping (until every tree is a star) and hooking
+    //     (each subgraph edge whose ends carry different labels links the
+    //     larger label under the smaller), until no edge joins two labels.
+    for (uint32_t x = tid; x < G * n; x += T) XL[x] = x % n;
+    __syncthreads();
+    for (uint32_t s = tid; s < n; s += T) {
+      const uint32_t d = XD[s];
+      if (!d) continue;
+      const uint32_t e1 = rp[s + 1];
+      for (uint32_t e = rp[s]; e < e1; ++e) {
+        const uint32_t j = col(e);
+        if (j >= s) continue;  // only this thread writes row s of every label array
+        uint32_t m = d & XD[j];
+        while (m) {
+          const uint32_t b = __ffs(m) - 1;
+          m &= m - 1;
+          uint32_t* l = XL + X.gidx[b] * n + s;
+          if (j < *l) *l = j;
+        }
       }
     }
-  }
-  __syncthreads();
-  for (uint32_t g = 0; g < G; ++g)
-    for (uint32_t s = tid; s < n; s += T) X.L[g * n + s] = uf_find(X.L + g * n, s);
-  __syncthreads();
-  for (uint32_t s = tid; s < n; s += T) {
-    const uint32_t d = X.D[s];
-    if (!d) continue;
-    const uint32_t e1 = F.rp[s + 1];
-    for (uint32_t e = F.rp[s]; e < e1; ++e) {
-      const uint32_t j = F.ent[e].x;
-      if (j <= s) continue;  // every undirected edge once; self-loops skipped
-      uint32_t m = d & X.D[j];
-      while (m) {
-        const uint32_t b = __ffs(m) - 1;
-        m &= m - 1;
-        uint32_t* L = X.L + X.gidx[b] * n;
-        if (L[s] != L[j]) uf_union(L, s, j);
+    __syncthreads();
+    if (pc) pc->lap(PHASE_ICM_INIT);
+    for (uint32_t round = 0; round <= n; ++round) {
+      for (uint32_t it = 0; it <= n; ++it) {
+        int ch = 0;
+        for (uint32_t x = tid; x < G * n; x += T) {
+          const uint32_t l = XL[x];
+          const uint32_t base = x - x % n;
+          const uint32_t ll = XL[base + l];
+          if (ll != l) {
+            XL[x] = ll;
+            ch = 1;
+          }
+        }
+        if (!__syncthreads_or(ch)) break;
       }
+      if (pc) pc->lap(PHASE_ICM_JUMP);
+      int ch = 0;
+      for (uint32_t s = tid; s < n; s += T) {
+        const uint32_t d = XD[s];
+        if (!d) continue;
+        const uint32_t e1 = rp[s + 1];
+        for (uint32_t e = rp[s]; e < e1; ++e) {
+          const uint32_t j = col(e);
+          if (j <= s) continue;  // every undirected edge once; self-loops skipped
+          uint32_t m = d & XD[j];
+          while (m) {
+            const uint32_t b = __ffs(m) - 1;
+            m &= m - 1;
+            uint32_t* L = XL + X.gidx[b] * n;
+            const uint32_t a = L[s], c = L[j];
+            if (a != c) {
+              atomicMin(L + max(a, c), min(a, c));
+              ch = 1;
+            }
+          }
+        }
+      }
+      const int any = __syncthreads_or(ch);
+      if (pc) pc->lap(PHASE_ICM_GROW);
+      if (!any) break;
     }
-  }
-  __syncthreads();
-  for (uint32_t g = 0; g < G; ++g)
-    for (uint32_t s = tid; s < n; s += T) X.L[g * n + s] = uf_find(X.L + g * n, s);
-  __syncthreads();
-  // root of every seed, then the cluster: q<0 sites in the seed's component
-  if (tid < 32 && ((gmask >> tid) & 1u) && X.cnt[tid]) X.seed[tid] = X.L[X.gidx[tid] * n + X.seed[tid]];
-  __syncthreads();
-  for (uint32_t s = tid; s < n; s += T) {
-    uint32_t d = X.D[s], c = 0;
-    while (d) {
-      const uint32_t b = __ffs(d) - 1;
-      d &= d - 1;
-      if (X.cnt[b] && X.L[X.gidx[b] * n + s] == X.seed[b]) c |= 1u << b;
+    // root of every seed, then the cluster: q<0 sites in the seed's component
+    if (tid < 32 && ((gmask >> tid) & 1u) && X.cnt[tid]) X.seed[tid] = XL[X.gidx[tid] * n + X.seed[tid]];
+    __syncthreads();
+    for (uint32_t s = tid; s < n; s += T) {
+      uint32_t d = XD[s], c = 0;
+      while (d) {
+        const uint32_t b = __ffs(d) - 1;
+        d &= d - 1;
+        if (X.cnt[b] && XL[X.gidx[b] * n + s] == X.seed[b]) c |= 1u << b;
+      }
+      XC[s] = c;
     }
-    X.Cl[s] = c;
+    __syncthreads();
+    if (pc) pc->lap(PHASE_ICM_MARK);
+  } else {
+    // BFS from the seeds of all slots, one level per barrier.  XC[s] holds the
+    // slots whose cluster contains s; a site is queued for the next level when
+    // it gains a slot bit (at most once per level: level marks), and listed
+    // in V the first time it gains any.  Frontier counters rotate over three
+    // entries so that one barrier per level separates reading, filling and
+    // clearing them.  A level runs only if the previous one added a (site,
+    // slot) pair, so the levels end within 32 n.
+    uint32_t* const F0 = XL;
+    uint32_t* const F1 = XL + n;
+    uint32_t* const V = XL + 2 * n;
+    uint32_t* const MK = XL + 3 * n;
+    if (tid < 32 && ((gmask >> tid) & 1u) && X.cnt[tid]) {
+      const uint32_t s0 = X.seed[tid];
+      const uint32_t old = atomicOr(&XC[s0], 1u << tid);
+      if (old == 0) V[atomicAdd(&X.q[3], 1u)] = s0;
+      if (atomicMax(&MK[s0], 1u) < 1u) F0[atomicAdd(&X.q[0], 1u)] = s0;
+    }
+    __syncthreads();
+    // Each frontier site is expanded by a team of BFS_LANES lanes (one edge
+    // each per step), and the appends to the next frontier and to V are
+    // aggregated per warp (one shared atomic per warp and step).
+    constexpr uint32_t BFS_LANES = 4;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (uint32_t lvl = 0; lvl < 32u * n + 2u; ++lvl) {
+      const uint32_t ncur = X.q[lvl % 3u];
+      if (ncur == 0) break;
+      const uint32_t* cur = (lvl & 1u) ? F1 : F0;
+      uint32_t* nxt = (lvl & 1u) ? F0 : F1;
+      uint32_t* qn = &X.q[(lvl + 1u) % 3u];
+      const uint32_t mark = lvl + 2u;
+      const uint32_t items = ncur * BFS_LANES;
+      for (uint32_t base = warp * 32u; base < items; base += T) {  // warp-uniform trip count
+        const uint32_t x = base + lane;
+        uint32_t c = 0, e = 0, e1 = 0;
+        if (x < items) {
+          const uint32_t s = cur[x / BFS_LANES];
+          c = XC[s];
+          e = rp[s] + x % BFS_LANES;
+          e1 = rp[s + 1];
+        }
+        const uint32_t steps = __reduce_max_sync(0xffffffffu, e < e1 ? (e1 - e + BFS_LANES - 1) / BFS_LANES : 0u);
+        for (uint32_t r = 0; r < steps; ++r, e += BFS_LANES) {
+          uint32_t j = 0;
+          bool pq = false, pv = false;
+          if (e < e1) {
+            j = col(e);
+            const uint32_t nb = c & XD[j] & ~XC[j];
+            if (nb) {
+              const uint32_t old = atomicOr(&XC[j], nb);
+              if (nb & ~old) {
+                pv = old == 0;
+                pq = atomicMax(&MK[j], mark) < mark;
+              }
+            }
+          }
+          const uint32_t bq = __ballot_sync(0xffffffffu, pq), bv = __ballot_sync(0xffffffffu, pv);
+          uint32_t oq = 0, ov = 0;
+          if (lane == 0) {
+            if (bq) oq = atomicAdd(qn, (uint32_t)__popc(bq));
+            if (bv) ov = atomicAdd(&X.q[3], (uint32_t)__popc(bv));
+          }
+          oq = __shfl_sync(0xffffffffu, oq, 0);
+          ov = __shfl_sync(0xffffffffu, ov, 0);
+          if (pq) nxt[oq + __popc(bq & lt)] = j;
+          if (pv) V[ov + __popc(bv & lt)] = j;
+        }
+      }
+      if (tid == 0) X.q[(lvl + 2u) % 3u] = 0;
+      __syncthreads();
+    }
+    vlist = V;
+    if (pc) pc->lap(PHASE_ICM_GROW);
   }
-  __syncthreads();
+  const uint32_t nlist = uf ? n : X.q[3];
   // energy change of flipping each cluster in both replicas: boundary terms
   // -2 s_i (h_i + sum_{j not in cluster} J_ij s_j), f32 per site, summed in
-  // fixed point per slot: each warp reduces by shuffles, warps combine in a
-  // fixed order (no shared-memory 64-bit atomics)
-  for (uint32_t gm = gmask; gm;) {
-    const uint32_t b = __ffs(gm) - 1;
-    gm &= gm - 1;
-    long long a0 = 0, a1 = 0;
-    if (X.cnt[b]) {
-      for (uint32_t s = tid; s < n; s += T) {
-        if (!((X.Cl[s] >> b) & 1u)) continue;
-        const float h = F.bias[s];
-        float f0 = h, f1 = h;
-        const uint32_t e1 = F.rp[s + 1];
-        for (uint32_t e = F.rp[s]; e < e1; ++e) {
-          const uint2 ce = F.ent[e];
-          if (ce.x == s || ((X.Cl[ce.x] >> b) & 1u)) continue;
-          const float Jv = __uint_as_float(ce.y);
-          f0 += ((W[ce.x * J.nw + o0] >> b) & 1u) ? -Jv : Jv;
-          f1 += ((W[ce.x * J.nw + o1] >> b) & 1u) ? -Jv : Jv;
+  // fixed point per slot.  The slots are dealt to teams of warps (all warps
+  // for one slot, one warp per slot for many); each warp reduces by shuffles
+  // and a team combines its warps in a fixed order.
+  {
+    const uint32_t team = max(1u, nwarp / G), teams = nwarp / team;
+    const uint32_t tw = warp % team, tid_team = warp / team;
+    const uint32_t iters = (G + teams - 1) / teams;
+    for (uint32_t it = 0; it < iters; ++it) {
+      const uint32_t g = it * teams + tid_team;
+      long long a0 = 0, a1 = 0;
+      uint32_t b = 32;
+      if (g < G && tid_team < teams) {
+        b = __fns(gmask, 0, (int)g + 1);
+        if (X.cnt[b]) {
+          for (uint32_t x = tw * 32 + lane; x < nlist; x += team * 32) {
+            const uint32_t s = vlist ? vlist[x] : x;
+            if (!((XC[s] >> b) & 1u)) continue;
+            const float h = bias[s];
+            float f0 = h, f1 = h;
+            const uint32_t e1 = rp[s + 1];
+            for (uint32_t e = rp[s]; e < e1; ++e) {
+              const uint2 ce = ent[e];
+              if (ce.x == s || ((XC[ce.x] >> b) & 1u)) continue;
+              const float Jv = __uint_as_float(ce.y);
+              f0 += ((r0(ce.x) >> b) & 1u) ? -Jv : Jv;
+              f1 += ((r1(ce.x) >> b) & 1u) ? -Jv : Jv;
+            }
+            const float s0 = ((r0(s) >> b) & 1u) ? -1.0f : 1.0f;
+            const float s1 = ((r1(s) >> b) & 1u) ? -1.0f : 1.0f;
+            a0 += to_fx(-2.0f * s0 * f0);
+            a1 += to_fx(-2.0f * s1 * f1);
+          }
         }
-        const float s0 = ((W[s * J.nw + o0] >> b) & 1u) ? -1.0f : 1.0f;
-        const float s1 = ((W[s * J.nw + o1] >> b) & 1u) ? -1.0f : 1.0f;
-        a0 += to_fx(-2.0f * s0 * f0);
-        a1 += to_fx(-2.0f * s1 * f1);
       }
+      for (int off = 16; off > 0; off >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+      }
+      if (lane == 0) {
+        X.part[warp * 2] = a0;
+        X.part[warp * 2 + 1] = a1;
+      }
+      __syncthreads();
+      if (tw == 0 && lane < 2 && b < 32 && X.cnt[b]) {
+        long long t = 0;
+        for (uint32_t k = 0; k < team; ++k) t += X.part[(warp + k) * 2 + lane];
+        X.dE[lane * 32 + b] = (unsigned long long)t;
+      }
+      __syncthreads();
     }
-    for (int off = 16; off > 0; off >>= 1) {
-      a0 += __shfl_xor_sync(0xffffffffu, a0, off);
-      a1 += __shfl_xor_sync(0xffffffffu, a1, off);
-    }
-    if (lane == 0) {
-      X.part[warp * 2] = a0;
-      X.part[warp * 2 + 1] = a1;
-    }
-    __syncthreads();
-    if (tid < 2) {
-      long long t = 0;
-      for (uint32_t k = 0; k < nwarp; ++k) t += X.part[k * 2 + tid];
-      X.dE[tid * 32 + b] = (unsigned long long)t;
-    }
-    __syncthreads();
   }
-  for (uint32_t s = tid; s < n; s += T) {
-    const uint32_t c = X.Cl[s];
+  for (uint32_t x = tid; x < nlist; x += T) {
+    const uint32_t s = vlist ? vlist[x] : x;
+    const uint32_t c = XC[s];
     if (c) {
-      atomicXor(&W[s * J.nw + o0], c);
-      atomicXor(&W[s * J.nw + o1], c);
+      atomicXor(&W[s * nw + o0], c);
+      atomicXor(&W[s * nw + o1], c);
     }
   }
 }
@@ -460,9 +573,9 @@ __device__ void icm_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i
           m &= m - 1;
         }
         lomask &= ~gmask;
-        icm_group(J, F, S.W, S.X, i, p, w, gmask);
+        icm_group(J, F, S.W, S.X, i, p, w, gmask, nullptr, nullptr, &pc);
         __syncthreads();
-        pc.lap(PHASE_ICM_GROW);
+        pc.lap(PHASE_ICM_APPLY);
         if (tid < 32 && ((gmask >> tid) & 1u) && S.X.cnt[tid]) {
           // the reference invalidates both caches; the next energy() is energy_ref
           const uint32_t x0 = c0 * J.ntp + tb + tid, x1 = c1 * J.ntp + tb + tid;
@@ -747,10 +860,22 @@ __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32
   __syncthreads();
 }
 
+// Copy of the job descriptor in shared memory: the phase functions read its
+// fields inside their loops, and shared-memory loads stay short where global
+// reloads of a descriptor evicted from L1 would go to L2.
+__device__ __forceinline__ void load_job(PtJob& dst, const PtJob* src) {
+  static_assert(sizeof(PtJob) % 8 == 0, "job descriptor copied as 8-byte words");
+  const uint2* a = reinterpret_cast<const uint2*>(src);
+  uint2* b = reinterpret_cast<uint2*>(&dst);
+  for (uint32_t x = threadIdx.x; x < sizeof(PtJob) / 8; x += blockDim.x) b[x] = a[x];
+  __syncthreads();
+}
+
 template <bool SELF>
 __device__ void run_job(const PtJob& J, char* smem_base) {
   Smem S;
-  carve_all(&S, smem_base, J.n, J.nw, J.C, J.ntp, J.qps, blockDim.x, J.F.nnz, J.csr_smem != 0, J.icm_group);
+  carve_all(&S, smem_base, J.n, J.nw, J.C, J.ntp, J.qps, blockDim.x, J.F.nnz, J.csr_smem != 0, J.icm_group,
+            J.icm_uf != 0);
   const uint32_t tid = threadIdx.x, T = blockDim.x;
   const uint32_t n = J.n;
   FastInst F = J.F;
@@ -817,15 +942,16 @@ __device__ void run_job(const PtJob& J, char* smem_base) {
 __global__ void __launch_bounds__(512, 1) k_pt_fused(const PtJob* __restrict__ jobs, uint32_t njobs, uint32_t* ctr) {
   extern __shared__ uint4 smem_u4[];
   __shared__ uint32_t s_job;
+  __shared__ PtJob s_J;
   for (;;) {
     if (threadIdx.x == 0) s_job = atomicAdd(ctr, 1u);
     __syncthreads();
     const uint32_t jid = s_job;
     __syncthreads();
     if (jid >= njobs) break;
-    const PtJob J = jobs[jid];
-    if (J.self_loops) run_job<true>(J, reinterpret_cast<char*>(smem_u4));
-    else run_job<false>(J, reinterpret_cast<char*>(smem_u4));
+    load_job(s_J, jobs + jid);
+    if (s_J.self_loops) run_job<true>(s_J, reinterpret_cast<char*>(smem_u4));
+    else run_job<false>(s_J, reinterpret_cast<char*>(smem_u4));
   }
 }
 
@@ -850,7 +976,9 @@ __host__ __device__ inline size_t plain_head_smem(uint32_t n, uint32_t C, uint32
 __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict__ jp, PlainCtl* ctl,
                                                        long long* acc, int mode) {
   extern __shared__ uint4 smem_u4[];
-  const PtJob J = *jp;
+  __shared__ PtJob s_J;
+  load_job(s_J, jp);
+  const PtJob& J = s_J;
   const uint32_t tid = threadIdx.x;
   char* base = reinterpret_cast<char*>(smem_u4);
   Smem S{};
@@ -900,15 +1028,32 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
 
 // Houdayer moves of round ctl->i: one CTA per (chain pair, slot >= lo).
 __global__ void __launch_bounds__(512) k_plain_icm(const PtJob* __restrict__ jp, const PlainCtl* __restrict__ ctl,
-                                                    long long* icm_dE, uint32_t* icm_valid) {
+                                                    long long* icm_dE, uint32_t* icm_valid, int stage_adj) {
   extern __shared__ uint4 smem_u4[];
-  const PtJob& J = *jp;
+  __shared__ PtJob s_J;
+  load_job(s_J, jp);
+  const PtJob& J = s_J;
   const uint32_t nact = J.nt - J.lo;
   const uint32_t p = blockIdx.x / nact, t = J.lo + blockIdx.x % nact;
+  char* base = reinterpret_cast<char*>(smem_u4);
   IcmScratch X;
-  carve_icm(&X, reinterpret_cast<char*>(smem_u4), 0, J.n, 1);
+  const size_t o = carve_icm(&X, base, 0, J.n, 1, J.icm_uf != 0);
+  FastInst F = J.F;
+  const uint16_t* cols = nullptr;
+  uint32_t* wstage = reinterpret_cast<uint32_t*>(base + o);  // [2][n] the pair's replica words
+  const size_t o2 = o + al16((size_t)2 * J.n * 4);
+  if (stage_adj) {
+    // row pointers and 16-bit column indices in shared memory for the cluster search
+    uint32_t* rp = reinterpret_cast<uint32_t*>(base + o2);
+    uint16_t* cl = reinterpret_cast<uint16_t*>(base + o2 + al16((size_t)(J.n + 1) * 4));
+    for (uint32_t x = threadIdx.x; x <= J.n; x += blockDim.x) rp[x] = J.F.rp[x];
+    for (uint32_t x = threadIdx.x; x < J.F.nnz; x += blockDim.x) cl[x] = (uint16_t)J.F.ent[x].x;
+    __syncthreads();
+    F.rp = rp;
+    cols = cl;
+  }
   const uint32_t b = t & 31u;
-  icm_group(J, J.F, J.W, X, ctl->i, p, t >> 5, 1u << b);
+  icm_group(J, F, J.W, X, ctl->i, p, t >> 5, 1u << b, cols, wstage);
   __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t x0 = 2 * p * J.ntp + t, x1 = (2 * p + 1) * J.ntp + t;
@@ -925,7 +1070,9 @@ __global__ void __launch_bounds__(512) k_plain_icm(const PtJob* __restrict__ jp,
 __global__ void __launch_bounds__(1024, 1) k_plain_exch(const PtJob* __restrict__ jp, PlainCtl* ctl,
                                                        const long long* icm_dE, uint32_t* icm_valid) {
   extern __shared__ uint4 smem_u4[];
-  const PtJob J = *jp;
+  __shared__ PtJob s_J;
+  load_job(s_J, jp);
+  const PtJob& J = s_J;
   const uint32_t tid = threadIdx.x;
   char* base = reinterpret_cast<char*>(smem_u4);
   Smem S{};
@@ -987,13 +1134,17 @@ __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ j
   const uint32_t wo = ch * J.wpc + (q >> 3), shift = 4 * (q & 7u);
   const float4 bl2 = b4[k];
   const FastInst F = J.F;
+  const uint2 key = J.key;
+  uint32_t* const W = J.W;
+  const uint32_t nw = J.nw;
+  const uint64_t s_first = gtid / J.qps, s_step = gstride / J.qps;
   Fx4 a{0, 0, 0, 0}, aq{0, 0, 0, 0};
-  for (uint64_t site = gtid / J.qps; site < nc; site += gstride / J.qps) {
+  for (uint64_t site = s_first; site < nc; site += s_step) {
     const uint32_t s = c0 + (uint32_t)site;
-    const uint4 rnd = philox4x32_10(make_uint4(s, i, ch * 16u + q, PTAG_SWEEP), J.key);
-    const uint32_t m = quad_update<true>(s, shift, F, J.W, J.nw, wo, bl2, rnd, a);
+    const uint4 rnd = philox4x32_10(make_uint4(s, i, ch * 16u + q, PTAG_SWEEP), key);
+    const uint32_t m = quad_update<true>(s, shift, F, W, nw, wo, bl2, rnd, a);
     if (m) {
-      atomicXor(&J.W[s * J.nw + wo], m << shift);
+      atomicXor(&W[s * nw + wo], m << shift);
       if (SELF) {
         const long long k2 = to_fx(2.0f * F.kd[s]);
         aq.x += (m & 1u) ? k2 : 0;
@@ -1062,7 +1213,7 @@ __global__ void k_plain_energy(const PtJob* __restrict__ jp, long long* acc) {
 }  // namespace
 
 size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem) {
-  return carve_all(nullptr, nullptr, j.n, j.nw, j.C, j.ntp, j.qps, T, j.F.nnz, csr_smem, j.icm_group);
+  return carve_all(nullptr, nullptr, j.n, j.nw, j.C, j.ntp, j.qps, T, j.F.nnz, csr_smem, j.icm_group, j.icm_uf != 0);
 }
 
 int fused_blocks_per_sm(uint32_t T, size_t smem) {
@@ -1080,15 +1231,21 @@ void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long 
   TAMC_CUDA(cudaGetLastError());
 }
 
-size_t plain_icm_bytes(const PtJob& j) { return carve_icm(nullptr, nullptr, 0, j.n, 1); }
+size_t plain_icm_bytes(const PtJob& j) {
+  return carve_icm(nullptr, nullptr, 0, j.n, 1, j.icm_uf != 0) + al16((size_t)2 * j.n * 4);
+}
+static size_t plain_icm_staged_bytes(const PtJob& j) {
+  return plain_icm_bytes(j) + al16((size_t)(j.n + 1) * 4) + al16((size_t)j.F.nnz * 2);
+}
 
 void plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, long long* icm_dE,
-                      uint32_t* icm_valid) {
+                      uint32_t* icm_valid, size_t smem_limit) {
   const uint32_t nact = j.nt - j.lo, grid = (j.C / 2) * nact;
   if (!j.icm || grid == 0) return;
-  const size_t smem = plain_icm_bytes(j);
+  const int stage = j.n <= 65536 && plain_icm_staged_bytes(j) <= smem_limit;
+  const size_t smem = stage ? plain_icm_staged_bytes(j) : plain_icm_bytes(j);
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_icm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_plain_icm<<<grid, 512, smem, st>>>(d_job, ctl, icm_dE, icm_valid);
+  k_plain_icm<<<grid, 512, smem, st>>>(d_job, ctl, icm_dE, icm_valid, stage);
   TAMC_CUDA(cudaGetLastError());
 }
 

@@ -15,6 +15,7 @@ struct PtJob {
   int32_t icm, threaded, self_loops, csr_smem;
   int32_t init;        // 0: load state, 1: random spins + energies, 2: load spins + energies
   uint32_t icm_group;  // ICM slots labelled together (label arrays in shared memory)
+  int32_t icm_uf;      // cluster search: 0 = frontier BFS from the seeds, 1 = union-find labelling
   const float* betas;  // [ntp], padding slots have beta = 0
   uint2 key;
   uint32_t* W;         // [n][nw]
@@ -34,8 +35,8 @@ struct PtJob {
   uint64_t cost;       // sweeps * n * R, for longest-first ordering
 };
 
-enum { PHASE_ICM_SCAN, PHASE_ICM_GROW, PHASE_ICM_APPLY, PHASE_EXCH, PHASE_SWEEP, PHASE_MEASURE, PHASE_OTHER,
-       PHASE_N };
+enum { PHASE_ICM_SCAN, PHASE_ICM_INIT, PHASE_ICM_JUMP, PHASE_ICM_GROW, PHASE_ICM_MARK, PHASE_ICM_APPLY, PHASE_EXCH,
+       PHASE_SWEEP, PHASE_MEASURE, PHASE_OTHER, PHASE_N };
 
 // Shared-memory bytes the fused kernel needs for a job with T threads.
 size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem);
@@ -58,7 +59,7 @@ void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long 
 size_t plain_icm_bytes(const PtJob& j);
 // Houdayer moves of round ctl->i, one CTA per (chain pair, slot >= lo)
 void plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, long long* icm_dE,
-                      uint32_t* icm_valid);
+                      uint32_t* icm_valid, size_t smem_limit);
 // energies after ICM, exchange, spin permutation; advances ctl->i
 void plain_launch_exch(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, const long long* icm_dE,
                        uint32_t* icm_valid);
