@@ -201,6 +201,36 @@ int tamc_gpu_sa_run_device(tamc_inst* inst, const float* d_betas, uint32_t nbeta
 /* Bytes of device scratch tamc_gpu_sa_run_device needs beyond its arguments. */
 uint64_t tamc_gpu_sa_scratch_bytes(tamc_inst* inst, uint32_t num_replicas);
 
+/* Largest replica-word scratch tamc_gpu_sa_run_noalloc accepts:
+ * ceil(num_replicas / 32) * n * 4 bytes must not exceed it (4 MiB: e.g. 1024
+ * replicas of up to 32768 spins). */
+#define TAMC_SA_NOALLOC_SCRATCH_BYTES (4u << 20)
+/* Simulated annealing in TAMC_MODE_FAST that allocates no device memory.
+ * No reference counterpart: it returns what tamc_gpu_sa_run (TAMC_MODE_FAST)
+ * returns -- energies_out as d_energies (float[num_replicas]) and packed_out as
+ * d_packed ([num_replicas][ceil(n/8)] bytes, the AnnealState layout) -- but
+ * into caller-owned device buffers, with d_betas (float[nbeta]) on the device.
+ *
+ * For callers that cannot allocate device memory mid-run: a serving loop
+ * that admits work against a fixed HBM budget (an allocation outside the
+ * budget defeats the admission), and host code on a latency path that must
+ * not meet the device-wide synchronisation cudaMalloc/cudaFree can cause.
+ * tamc_gpu_sa_run allocates its replica words on first use; this entry point
+ * uses a file-scope device array of TAMC_SA_NOALLOC_SCRATCH_BYTES instead and
+ * fails with TAMC_E_INVAL for larger num_replicas x n.
+ *
+ * First call on a device: resolves the array's address on that device
+ * (cudaGetSymbolAddress, with the context's device made current); make one
+ * call per device before any stream capture begins.  Each call clears the
+ * words it uses (cudaMemsetAsync on `stream`) before the anneal, so nothing
+ * has to be zero beforehand.  All calls on one device share the one array:
+ * calls whose work overlaps on the device (different streams, or threads
+ * that do not wait for each other) race on it; order them on one stream or
+ * synchronise between them.  Launches on `stream` (NULL = the context
+ * stream) and returns without waiting. */
+int tamc_gpu_sa_run_noalloc(tamc_inst* inst, const float* d_betas, uint32_t nbeta, uint32_t num_replicas,
+                            uint64_t seed, float* d_energies, uint8_t* d_packed, void* stream);
+
 /* ------------------------------------------------------------------------
  * Batched PT-ICM (TAMC_MODE_FAST): many instances of uneven N, ladder length
  * and chain count in one persistent kernel that pulls instance tiles from a

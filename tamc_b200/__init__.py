@@ -104,6 +104,7 @@ _SIGS = {
                                   u32p]),
     "tamc_gpu_sa_run_device": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint64, vp, vp, vp]),
     "tamc_gpu_sa_scratch_bytes": (C.c_uint64, [vp, C.c_uint32]),
+    "tamc_gpu_sa_run_noalloc": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint64, vp, vp, vp]),
     "tamc_gpu_batch_create": (C.c_int, [vp, C.POINTER(vp)]),
     "tamc_gpu_batch_add": (C.c_int, [vp, vp, C.POINTER(_PtParams), C.c_uint64, u32p]),
     "tamc_gpu_batch_run": (C.c_int, [vp]),
@@ -465,6 +466,19 @@ def sa_run_device(dinst: DeviceInstance, d_betas: int, nbeta: int, num_replicas:
     """Device-resident SA (all pointers are device addresses, e.g. torch tensor data_ptr())."""
     _check(lib().tamc_gpu_sa_run_device(dinst.h, d_betas, nbeta, num_replicas, seed, d_energies, d_words,
                                         stream or None))
+
+
+# largest ceil(num_replicas/32) * n * 4 that sa_run_noalloc accepts (TAMC_SA_NOALLOC_SCRATCH_BYTES)
+SA_NOALLOC_SCRATCH_BYTES = 4 << 20
+
+
+def sa_run_noalloc(dinst: DeviceInstance, d_betas: int, nbeta: int, num_replicas: int, seed: int, d_energies: int,
+                   d_packed: int, stream: int = 0) -> None:
+    """Fast-mode SA with no device allocation: energies and packed states into
+    caller-owned device buffers; replica words in a static device array shared
+    by all calls on the device (calls must not overlap)."""
+    _check(lib().tamc_gpu_sa_run_noalloc(dinst.h, d_betas, nbeta, num_replicas, seed, d_energies, d_packed,
+                                         stream or None))
 
 
 def unpack_bits(packed: np.ndarray, n: int) -> np.ndarray:

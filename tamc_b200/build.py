@@ -26,8 +26,8 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 GXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 GCC = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["ctx.cu", "ref_kernels.cu", "fast_sa.cu", "sa_api.cu", "pt.cu", "fast_pt.cu", "fast_host.cu",
-              "serve.cu"]
+CU_SOURCES = ["ctx.cu", "ref_kernels.cu", "fast_sa.cu", "sa_api.cu", "sa_noalloc.cu", "pt.cu", "fast_pt.cu",
+              "fast_host.cu", "serve.cu"]
 CPP_SOURCES = ["host_instance.cpp", "method.cpp", "writers.cpp"]
 HEADERS = ["device.cuh", "expf_exact.h", "internal.h", "fast_common.cuh", "fast_sa.cuh", "fast_pt.cuh", "pt.cuh",
            "ref_kernels.cuh"]

@@ -277,4 +277,13 @@ void sa_fast_launch(cudaStream_t st, const SaFastArgs& a, const SaTile& t) {
   }
 }
 
+SaTile sa_fast_peek(const tamc_gpu* g, const FastInst& F, uint32_t R) {
+  {
+    std::lock_guard<std::mutex> lk(g_sa_mu);
+    auto it = g_sa_tune.find(std::make_tuple(g->device, F.n, F.nnz, R));
+    if (it != g_sa_tune.end()) return it->second;
+  }
+  return heuristic(g, F, R);
+}
+
 }  // namespace tamc

@@ -26,5 +26,8 @@ SaTile sa_fast_choose(tamc_gpu* g, const FastInst& F, uint32_t R);
 // Device-side conversion of SA words to the reference's packed byte layout.
 void sa_pack_states(cudaStream_t st, const uint32_t* words, uint32_t n, uint32_t R, uint8_t* out);
 void sa_fast_launch(cudaStream_t st, const SaFastArgs& a, const SaTile& t);
+// The tile sa_fast_choose has cached for this shape, else the heuristic tile;
+// never times candidates, so it launches and allocates nothing.
+SaTile sa_fast_peek(const tamc_gpu* g, const FastInst& F, uint32_t R);
 
 }  // namespace tamc
