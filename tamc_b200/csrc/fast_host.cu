@@ -29,6 +29,7 @@ struct tamc_pt::FastState {
   tamc::DBuf<long long> eacc;  // fixed-point sweep sums (2 x C x ntp)
   tamc::DBuf<long long> icm_dE;     // fixed-point ICM energy changes (C x ntp)
   tamc::DBuf<uint32_t> icm_valid;   // caches invalidated by ICM (C x ntp)
+  tamc::DBuf<unsigned long long> dm;  // exchange: swapped slot pairs per chain
   size_t head_smem = 0;
   uint32_t grid_cap = 0;
   std::map<uint32_t, cudaGraphExec_t> graphs;  // captured chunks of K rounds
@@ -265,8 +266,9 @@ static void plain_enqueue_rounds(tamc_pt* pt, uint32_t K) {
   const auto& off = pt->inst->color_off;
   for (uint32_t r = 0; r < K; ++r) {
     plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem);
-    plain_launch_icm(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, pt->g->smem_optin);
-    plain_launch_exch(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p);
+    if (!plain_launch_icm(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, pt->g->smem_optin, F->dm.p))
+      plain_launch_exch(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, F->dm.p);
+    plain_launch_perm(st, j, F->d_job.p, F->dm.p, F->grid_cap);
     for (uint32_t c = 0; c + 1 < off.size(); ++c)
       plain_launch_sweep(st, j, F->d_job.p, F->ctl.p, c, (off[c + 1] - off[c]) * j.qps, F->eacc.p, F->grid_cap);
   }
@@ -306,6 +308,8 @@ static void plain_setup(tamc_pt* pt) {
   F->icm_dE.alloc((size_t)j.C * j.ntp);
   F->icm_valid.alloc((size_t)j.C * j.ntp);
   F->icm_valid.zero(st);
+  F->dm.alloc(j.C);
+  F->dm.zero(st);
   if (plain_icm_bytes(j) > pt->g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the plain ICM kernel");
   j.init = 0;
   j.count_out = nullptr;

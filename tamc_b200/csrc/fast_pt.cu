@@ -416,6 +416,59 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     }
     __syncthreads();
     if (pc) pc->lap(PHASE_ICM_MARK);
+  } else if (G == 1) {
+    // One slot: a site joins the cluster exactly once (the atomicOr that sets
+    // its bit tells which thread got there first), so the levels are
+    // consecutive segments of one queue V, which ends up listing the cluster.
+    // Counters rotate over three entries as in the multi-slot search below.
+    uint32_t* const V = XL;
+    const uint32_t b = __ffs(gmask) - 1, bit = 1u << b;
+    if (tid == 0 && X.cnt[b]) {
+      XC[X.seed[b]] = bit;
+      V[0] = X.seed[b];
+      X.q[0] = 1;
+    }
+    __syncthreads();
+    constexpr uint32_t BFS_LANES = 4;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t lo = 0;
+    for (uint32_t lvl = 0; lvl < n + 2u; ++lvl) {
+      const uint32_t ncur = X.q[lvl % 3u];
+      if (ncur == 0) break;
+      uint32_t* qn = &X.q[(lvl + 1u) % 3u];
+      uint32_t* nxt = V + lo + ncur;
+      const uint32_t items = ncur * BFS_LANES;
+      for (uint32_t base = warp * 32u; base < items; base += T) {  // warp-uniform trip count
+        const uint32_t x = base + lane;
+        uint32_t e = 0, e1 = 0;
+        if (x < items) {
+          const uint32_t s = V[lo + x / BFS_LANES];
+          e = rp[s] + x % BFS_LANES;
+          e1 = rp[s + 1];
+        }
+        const uint32_t steps = __reduce_max_sync(0xffffffffu, e < e1 ? (e1 - e + BFS_LANES - 1) / BFS_LANES : 0u);
+        for (uint32_t r = 0; r < steps; ++r, e += BFS_LANES) {
+          uint32_t j = 0;
+          bool pq = false;
+          if (e < e1) {
+            j = col(e);
+            if ((XD[j] & bit) && !(XC[j] & bit)) pq = !(atomicOr(&XC[j], bit) & bit);
+          }
+          const uint32_t bq = __ballot_sync(0xffffffffu, pq);
+          uint32_t oq = 0;
+          if (lane == 0 && bq) oq = atomicAdd(qn, (uint32_t)__popc(bq));
+          oq = __shfl_sync(0xffffffffu, oq, 0);
+          if (pq) nxt[oq + __popc(bq & lt)] = j;
+        }
+      }
+      lo += ncur;
+      if (tid == 0) X.q[(lvl + 2u) % 3u] = 0;
+      __syncthreads();
+    }
+    if (tid == 0) X.q[3] = lo;
+    __syncthreads();
+    vlist = V;
+    if (pc) pc->lap(PHASE_ICM_GROW);
   } else {
     // BFS from the seeds of all slots, one level per barrier.  XC[s] holds the
     // slots whose cluster contains s; a site is queued for the next level when
@@ -591,8 +644,11 @@ __device__ void icm_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i
   }
 }
 
-__device__ void exchange_phase(const PtJob& J, Smem& S, uint32_t i) {
-  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
+// Exchange decisions of round i (threaded or serial semantics), acceptance
+// counts, the slot permutation of energies and tags, round trips; S.Dm[c]
+// receives the swapped pairs of chain c.
+__device__ void exchange_decide(const PtJob& J, Smem& S, uint32_t i) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const uint32_t nt = J.nt;
   for (uint32_t c = warp; c < J.C; c += nwarp) {
     double* Ec = S.Ec + c * J.ntp;
@@ -676,7 +732,18 @@ __device__ void exchange_phase(const PtJob& J, Smem& S, uint32_t i) {
     if (lane == 0) S.Dm[c] = D;
   }
   __syncthreads();
-  // move the spins: one bit permutation per chain word
+}
+
+__device__ void permute_words(const PtJob& J, Smem& S);
+__device__ __forceinline__ void exchange_phase(const PtJob& J, Smem& S, uint32_t i) {
+  exchange_decide(J, S, i);
+  permute_words(J, S);
+}
+
+// Moves the spins after the exchange decisions: one bit permutation per chain
+// word (Dm[c] marks the swapped slot pairs of chain c).
+__device__ void permute_words(const PtJob& J, Smem& S) {
+  const uint32_t tid = threadIdx.x;
   for (uint32_t s = tid; s < J.n; s += blockDim.x) {
     for (uint32_t c = 0; c < J.C; ++c) {
       const uint64_t D = S.Dm[c];
@@ -1026,9 +1093,12 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
   }
 }
 
+__device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long long* icm_dE, uint32_t* icm_valid,
+                                    char* base, unsigned long long* dm);
+
 // Houdayer moves of round ctl->i: one CTA per (chain pair, slot >= lo).
-__global__ void __launch_bounds__(512) k_plain_icm(const PtJob* __restrict__ jp, const PlainCtl* __restrict__ ctl,
-                                                    long long* icm_dE, uint32_t* icm_valid, int stage_adj) {
+__global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__ jp, PlainCtl* ctl, long long* icm_dE,
+                                                       uint32_t* icm_valid, int stage_adj, unsigned long long* dm) {
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -1053,7 +1123,9 @@ __global__ void __launch_bounds__(512) k_plain_icm(const PtJob* __restrict__ jp,
     cols = cl;
   }
   const uint32_t b = t & 31u;
-  icm_group(J, F, J.W, X, ctl->i, p, t >> 5, 1u << b, cols, wstage);
+  PhaseClock pc;  // with profiling on, cycles are summed over the CTAs
+  pc.start(J.prof);
+  icm_group(J, F, J.W, X, ctl->i, p, t >> 5, 1u << b, cols, wstage, &pc);
   __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t x0 = 2 * p * J.ntp + t, x1 = (2 * p + 1) * J.ntp + t;
@@ -1063,18 +1135,28 @@ __global__ void __launch_bounds__(512) k_plain_icm(const PtJob* __restrict__ jp,
     icm_dE[x0] = (long long)X.dE[b];
     icm_dE[x1] = (long long)X.dE[32 + b];
   }
+  pc.lap(PHASE_ICM_APPLY);
+  // the last CTA to finish runs the exchange of the round (no waiting: the
+  // others have published their results before counting themselves done)
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctl->icm_done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) ctl->icm_done = 0;
+  plain_exchange_body(J, ctl, icm_dE, icm_valid, base, dm);
 }
 
-// Energies after the Houdayer moves, replica exchange and the spin permutation
-// of round ctl->i; then the sweeps of that round may run.
-__global__ void __launch_bounds__(1024, 1) k_plain_exch(const PtJob* __restrict__ jp, PlainCtl* ctl,
-                                                       const long long* icm_dE, uint32_t* icm_valid) {
-  extern __shared__ uint4 smem_u4[];
-  __shared__ PtJob s_J;
-  load_job(s_J, jp);
-  const PtJob& J = s_J;
+// Energies after the Houdayer moves and the exchange decisions of round
+// ctl->i (the spin permutation follows in k_plain_perm); advances ctl->i.
+// `base` is shared memory for Ec, Er and Dm; dm receives Dm for k_plain_perm.
+__device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long long* icm_dE, uint32_t* icm_valid,
+                                    char* base, unsigned long long* dm) {
   const uint32_t tid = threadIdx.x;
-  char* base = reinterpret_cast<char*>(smem_u4);
   Smem S{};
   S.Ec = (double*)base;
   S.Er = (double*)(base + al16((size_t)J.C * J.ntp * 8));
@@ -1083,8 +1165,9 @@ __global__ void __launch_bounds__(1024, 1) k_plain_exch(const PtJob* __restrict_
   const uint32_t CN = J.C * J.ntp;
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
     double ec = J.Ec[x], er = J.Er[x];
-    if (J.icm && icm_valid[x]) {  // invalidated caches are recomputed as energy_ref
-      er += (double)icm_dE[x] * TAMC_FX_INV;
+    // written by other CTAs of the Houdayer kernel: read through L2
+    if (J.icm && __ldcg(icm_valid + x)) {  // invalidated caches are recomputed as energy_ref
+      er += (double)__ldcg(icm_dE + x) * TAMC_FX_INV;
       ec = er;
       icm_valid[x] = 0;
     }
@@ -1095,16 +1178,47 @@ __global__ void __launch_bounds__(1024, 1) k_plain_exch(const PtJob* __restrict_
   PhaseClock pc;
   pc.start(J.prof);
   const uint32_t i = ctl->i;
-  exchange_phase(J, S, i);
+  exchange_decide(J, S, i);
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
     J.Ec[x] = S.Ec[x];
     J.Er[x] = S.Er[x];
   }
+  for (uint32_t c = tid; c < J.C; c += blockDim.x) dm[c] = S.Dm[c];
   __syncthreads();
   pc.lap(PHASE_EXCH);
   if (tid == 0) {
     ctl->i = i + 1;
     ctl->pending = 1;
+  }
+}
+
+// Exchange of round ctl->i when no Houdayer kernel ran (icm off, or no slot >= lo).
+__global__ void __launch_bounds__(1024, 1) k_plain_exch(const PtJob* __restrict__ jp, PlainCtl* ctl,
+                                                       const long long* icm_dE, uint32_t* icm_valid,
+                                                       unsigned long long* dm) {
+  extern __shared__ uint4 smem_u4[];
+  __shared__ PtJob s_J;
+  load_job(s_J, jp);
+  plain_exchange_body(s_J, ctl, icm_dE, icm_valid, reinterpret_cast<char*>(smem_u4), dm);
+}
+
+// Spin permutation of the exchange: one thread per (site, chain) word pair.
+__global__ void __launch_bounds__(256) k_plain_perm(const PtJob* __restrict__ jp, const unsigned long long* dm) {
+  const PtJob& J = *jp;
+  const uint32_t C = J.C, wpc = J.wpc, nw = J.nw;
+  uint32_t* const W = J.W;
+  const uint64_t total = (uint64_t)J.n * C;
+  for (uint64_t x = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+       x += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = (uint32_t)(x / C), c = (uint32_t)(x % C);
+    const uint64_t D = dm[c];
+    if (!D) continue;
+    uint32_t* w = W + (size_t)s * nw + c * wpc;
+    uint64_t v = w[0];
+    if (wpc > 1) v |= (uint64_t)w[1] << 32;
+    v = bitperm(v, D);
+    w[0] = (uint32_t)v;
+    if (wpc > 1) w[1] = (uint32_t)(v >> 32);
   }
 }
 
@@ -1238,22 +1352,31 @@ static size_t plain_icm_staged_bytes(const PtJob& j) {
   return plain_icm_bytes(j) + al16((size_t)(j.n + 1) * 4) + al16((size_t)j.F.nnz * 2);
 }
 
-void plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, long long* icm_dE,
-                      uint32_t* icm_valid, size_t smem_limit) {
+bool plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, long long* icm_dE,
+                      uint32_t* icm_valid, size_t smem_limit, unsigned long long* dm) {
   const uint32_t nact = j.nt - j.lo, grid = (j.C / 2) * nact;
-  if (!j.icm || grid == 0) return;
+  if (!j.icm || grid == 0) return false;
   const int stage = j.n <= 65536 && plain_icm_staged_bytes(j) <= smem_limit;
-  const size_t smem = stage ? plain_icm_staged_bytes(j) : plain_icm_bytes(j);
+  const size_t smem = std::max(stage ? plain_icm_staged_bytes(j) : plain_icm_bytes(j), plain_head_smem(j.n, j.C, j.ntp));
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_icm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_plain_icm<<<grid, 512, smem, st>>>(d_job, ctl, icm_dE, icm_valid, stage);
+  k_plain_icm<<<grid, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, stage, dm);
   TAMC_CUDA(cudaGetLastError());
+  return true;
 }
 
 void plain_launch_exch(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, const long long* icm_dE,
-                       uint32_t* icm_valid) {
+                       uint32_t* icm_valid, unsigned long long* dm) {
   const size_t smem = plain_head_smem(j.n, j.C, j.ntp);
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_exch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_plain_exch<<<1, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid);
+  k_plain_exch<<<1, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, dm);
+  TAMC_CUDA(cudaGetLastError());
+}
+
+void plain_launch_perm(cudaStream_t st, const PtJob& j, const PtJob* d_job, const unsigned long long* dm,
+                       uint32_t grid_cap) {
+  const uint64_t total = (uint64_t)j.n * j.C;
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(grid_cap, (total + 255) / 256));
+  k_plain_perm<<<grid, 256, 0, st>>>(d_job, dm);
   TAMC_CUDA(cudaGetLastError());
 }
 
