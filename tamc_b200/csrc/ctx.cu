@@ -76,7 +76,7 @@ void tamc_inst_release(tamc_inst* d) {
   tamc_gpu* g = d->g;
   cudaSetDevice(g->device);
   void* ptrs[] = {d->d_rp, d->d_col, d->d_J, d->d_bias, d->d_grp, d->d_gcol, d->d_sus, d->d_color_off,
-                  d->d_perm, d->d_iperm, d->d_frp, d->d_fent, d->d_fbias, d->d_fkd, d->d_fsus};
+                  d->d_perm, d->d_iperm, d->d_frp, d->d_fent, d->d_fcol16, d->d_fbias, d->d_fkd, d->d_fsus};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   d->sa_scratch.release();
@@ -218,6 +218,11 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
     d->d_iperm = dmalloc_copy(iperm.data(), iperm.size());
     d->d_frp = dmalloc_copy(frp.data(), frp.size());
     d->d_fent = dmalloc_copy(fent.data(), fent.size());
+    if (h.n <= 65536) {
+      std::vector<uint16_t> c16((fent.size() + 7) / 8 * 8 + 8, 0);
+      for (size_t e = 0; e < fent.size(); ++e) c16[e] = (uint16_t)fent[e].x;
+      d->d_fcol16 = dmalloc_copy(c16.data(), c16.size());
+    }
     d->d_fbias = dmalloc_copy(fbias.data(), fbias.size());
     d->d_fkd = dmalloc_copy(fkd.data(), fkd.size());
     d->d_fsus = dmalloc_copy(fsus.data(), fsus.size());

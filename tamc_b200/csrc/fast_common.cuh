@@ -20,6 +20,7 @@ struct FastInst {  // colour-ordered instance (device pointers)
   const uint32_t* iperm;      // original -> new
   const uint32_t* rp;         // n + 1
   const uint2* ent;           // nnz (new column, J bits)
+  const uint16_t* col16;      // nnz new column as 16 bits, padded to 8 entries; null if n > 65536
   const float* bias;          // n
   const float* kd;            // n self-loop coefficient
   const double* sus;          // [nchi][n], colour order

@@ -31,6 +31,7 @@ struct tamc_pt::FastState {
   tamc::DBuf<uint32_t> icm_valid;   // caches invalidated by ICM (C x ntp)
   tamc::DBuf<unsigned long long> dm;  // exchange: swapped slot pairs per chain
   size_t head_smem = 0;
+  int head_stage = 0;  // the head kernel stages replica words for measurements
   uint32_t grid_cap = 0;
   std::map<uint32_t, cudaGraphExec_t> graphs;  // captured chunks of K rounds
   tamc::DBuf<unsigned long long> prof;          // per-phase cycles (TAMC_PHASE_PROF=1)
@@ -265,14 +266,14 @@ static void plain_enqueue_rounds(tamc_pt* pt, uint32_t K) {
   cudaStream_t st = pt->g->stream;
   const auto& off = pt->inst->color_off;
   for (uint32_t r = 0; r < K; ++r) {
-    plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem);
+    plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem, F->head_stage);
     if (!plain_launch_icm(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, pt->g->smem_optin, F->dm.p))
       plain_launch_exch(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, F->dm.p);
     plain_launch_perm(st, j, F->d_job.p, F->dm.p, F->grid_cap);
     for (uint32_t c = 0; c + 1 < off.size(); ++c)
       plain_launch_sweep(st, j, F->d_job.p, F->ctl.p, c, (off[c + 1] - off[c]) * j.qps, F->eacc.p, F->grid_cap);
   }
-  plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem);  // close the last round
+  plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem, F->head_stage);  // close the last round
 }
 
 static void plain_run_chunk(tamc_pt* pt, uint32_t K) {
@@ -298,7 +299,8 @@ static void plain_setup(tamc_pt* pt) {
   PtJob& j = F->job;
   cudaStream_t st = pt->g->stream;
   F->plain = true;
-  F->head_smem = plain_head_bytes(j);
+  F->head_stage = plain_head_bytes(j, true) <= pt->g->smem_optin;
+  F->head_smem = plain_head_bytes(j, F->head_stage != 0);
   if (F->head_smem > pt->g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the plain PT head kernel");
   F->grid_cap = (uint32_t)pt->g->num_sms * 8;
   F->ctl.alloc(1);
@@ -321,7 +323,7 @@ static void plain_init_energies(tamc_pt* pt, bool random) {
   cudaStream_t st = pt->g->stream;
   F->eacc.zero(st);
   plain_launch_init(st, F->d_job.p, F->eacc.p, random ? 1 : 0, (uint32_t)pt->g->num_sms * 4);
-  plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 2, F->head_smem);
+  plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 2, F->head_smem, F->head_stage);
   pt->g->count(random ? 3 : 2);
   TAMC_CUDA(cudaStreamSynchronize(st));
 }
@@ -338,7 +340,7 @@ static bool choose_plain(tamc_pt* pt) {
   if (g_no_autotune) return fused_smem_bytes(pt->fast->job, 512, false) > pt->g->smem_optin;
   const PtJob& j = pt->fast->job;
   const bool fused_fits = fused_smem_bytes(j, 128, false) <= pt->g->smem_optin;
-  const bool plain_fits = plain_head_bytes(j) <= pt->g->smem_optin;
+  const bool plain_fits = plain_head_bytes(j, false) <= pt->g->smem_optin;
   if (!fused_fits || !plain_fits) return !fused_fits;
   const auto key = std::make_tuple(pt->g->device, j.n, j.F.nnz, j.nt, j.C, (int)j.icm_uf);
   {

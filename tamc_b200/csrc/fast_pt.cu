@@ -566,12 +566,20 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
             const float h = bias[s];
             float f0 = h, f1 = h;
             const uint32_t e1 = rp[s + 1];
-            for (uint32_t e = rp[s]; e < e1; ++e) {
-              const uint2 ce = ent[e];
-              if (ce.x == s || ((XC[ce.x] >> b) & 1u)) continue;
-              const float Jv = __uint_as_float(ce.y);
-              f0 += ((r0(ce.x) >> b) & 1u) ? -Jv : Jv;
-              f1 += ((r1(ce.x) >> b) & 1u) ? -Jv : Jv;
+            for (uint32_t e = rp[s]; e < e1; e += 8) {
+              // up to 8 entries loaded before use (independent loads in flight),
+              // then summed in row order
+              uint2 ce[8];
+#pragma unroll
+              for (uint32_t k = 0; k < 8; ++k)
+                if (e + k < e1) ce[k] = ent[e + k];
+#pragma unroll
+              for (uint32_t k = 0; k < 8; ++k) {
+                if (e + k >= e1 || ce[k].x == s || ((XC[ce[k].x] >> b) & 1u)) continue;
+                const float Jv = __uint_as_float(ce[k].y);
+                f0 += ((r0(ce[k].x) >> b) & 1u) ? -Jv : Jv;
+                f1 += ((r1(ce[k].x) >> b) & 1u) ? -Jv : Jv;
+              }
             }
             const float s0 = ((r0(s) >> b) & 1u) ? -1.0f : 1.0f;
             const float s1 = ((r1(s) >> b) & 1u) ? -1.0f : 1.0f;
@@ -832,15 +840,20 @@ __device__ __forceinline__ bool sched(int64_t period, uint32_t i, uint32_t meas_
   return period >= 0 && i >= meas_init && ((i - meas_init) % (uint32_t)period == 0 || i == num_sweeps - 1);
 }
 
-__device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i, uint32_t& m_cur,
-                              uint32_t& s_cur) {
-  __shared__ int s_new;
-  __shared__ uint32_t s_k, s_c, s_t;
-  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  const uint32_t n = J.n, nt = J.nt, C = J.C;
-  // ground-state tracking: the reference takes the first minimum over slots,
-  // then the first over chains (lexicographic (E, chain, slot)), and records
-  // it when strictly below the running minimum.  Warp 0 reduces.
+// A new running minimum found by gs_track: its log entry, chain and slot.
+struct GsSnap {
+  int fresh;
+  uint32_t k, c, t;
+};
+
+// Ground-state tracking (apply_measurements, src/pt.rs:542-583): the
+// reference takes the first minimum over slots, then the first over chains
+// (lexicographic (E, chain, slot)), and records it when strictly below the
+// running minimum.  Warp 0 reduces; every thread gets the result.
+__device__ GsSnap gs_track(const PtJob& J, Smem& S, uint32_t i) {
+  __shared__ GsSnap s_g;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t nt = J.nt, C = J.C;
   if (warp == 0) {
     float be = INFINITY;
     uint32_t bx = 0xffffffffu;
@@ -854,7 +867,7 @@ __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32
       if (oe < be || (oe == be && ox < bx)) { be = oe; bx = ox; }
     }
     if (lane == 0) {
-      s_new = 0;
+      GsSnap g{0, 0, 0, 0};
       if (!*J.log.have || be < *J.log.minE) {
         *J.log.have = 1;
         *J.log.minE = be;
@@ -862,24 +875,32 @@ __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32
         if (k < J.log.cap) {
           J.log.steps[k] = i;
           J.log.E[k] = be;
-          s_new = 1;
-          s_k = k;
-          s_c = bx / nt;
-          s_t = bx % nt;
+          g = GsSnap{1, k, bx / nt, bx % nt};
         }
         *J.log.count = k + 1;
       }
+      s_g = g;
     }
   }
   __syncthreads();
-  if (s_new) {
+  return s_g;
+}
+
+// The rest of a round's measurements, after gs_track: the new minimum's
+// state, and on the sampling schedule e / q / suscept (weights `sus`,
+// [nchi][n] in colour order) and packed state samples.
+__device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const double* sus, uint32_t i,
+                             uint32_t& m_cur, uint32_t& s_cur, GsSnap g) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  const uint32_t n = J.n, nt = J.nt, C = J.C;
+  if (g.fresh) {
     const uint32_t nw64 = (n + 63) / 64;
-    const uint32_t o = s_c * J.wpc + (s_t >> 5), b = s_t & 31u;
+    const uint32_t o = g.c * J.wpc + (g.t >> 5), b = g.t & 31u;
     for (uint32_t wd = tid; wd < nw64; wd += blockDim.x) {
       uint64_t v = 0;
       for (uint32_t x = 0; x < 64 && wd * 64 + x < n; ++x)
         v |= (uint64_t)((S.W[F.iperm[wd * 64 + x] * J.nw + o] >> b) & 1u) << x;
-      J.log.words[(size_t)s_k * nw64 + wd] = v;
+      J.log.words[(size_t)g.k * nw64 + wd] = v;
     }
   }
   const uint32_t P = C / 2;
@@ -897,7 +918,7 @@ __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32
       for (int off = 16; off > 0; off >>= 1) neg += __shfl_xor_sync(0xffffffffu, neg, off);
       if (lane == 0) J.out.q[(size_t)t * J.out.M * P + (size_t)m * P + p] = (int32_t)n - 2 * (int32_t)neg;
       for (uint32_t kx = 0; kx < J.out.nchi; ++kx) {
-        const double* wv = F.sus + (size_t)kx * n;
+        const double* wv = sus + (size_t)kx * n;
         double chi = 0.0;
         for (uint32_t s = lane; s < n; s += 32) {
           const uint32_t x = (S.W[s * J.nw + o0] ^ S.W[s * J.nw + o1]) >> b & 1u;
@@ -925,6 +946,12 @@ __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32
     }
   }
   __syncthreads();
+}
+
+__device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i, uint32_t& m_cur,
+                              uint32_t& s_cur) {
+  const GsSnap g = gs_track(J, S, i);
+  measure_rest(J, F, S, F.sus, i, m_cur, s_cur, g);
 }
 
 // Copy of the job descriptor in shared memory: the phase functions read its
@@ -1041,7 +1068,7 @@ __host__ __device__ inline size_t plain_head_smem(uint32_t n, uint32_t C, uint32
 // Close the previous round (add its fixed-point sweep sums, measurements), or
 // (mode 2) set the initial energies from the energy kernel's sums.
 __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict__ jp, PlainCtl* ctl,
-                                                       long long* acc, int mode) {
+                                                       long long* acc, int mode, int stage) {
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -1077,7 +1104,30 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
   pc.start(J.prof);
   if (pending) {
     const uint32_t ip = ctl->i - 1;
-    if (ip >= J.meas_init) measure_phase(J, F, S, ip, m_cur, s_cur);
+    if (ip >= J.meas_init) {
+      const GsSnap g = gs_track(J, S, ip);
+      const bool meas = sched(J.sample, ip, J.meas_init, J.num_sweeps);
+      const bool snap = sched(J.sample_states, ip, J.meas_init, J.num_sweeps);
+      const double* sus = F.sus;
+      if (stage && (g.fresh || meas || snap)) {
+        // the measurements gather bits of every site: read the replica words
+        // (and the weights) once into shared memory instead of from L2
+        char* st = base + plain_head_smem(J.n, J.C, J.ntp);
+        uint32_t* Ws = reinterpret_cast<uint32_t*>(st);
+        const uint32_t nwords = J.n * J.nw;
+        for (uint32_t x = tid; x < nwords / 4; x += blockDim.x)
+          reinterpret_cast<uint4*>(Ws)[x] = reinterpret_cast<const uint4*>(J.W)[x];
+        for (uint32_t x = nwords / 4 * 4 + tid; x < nwords; x += blockDim.x) Ws[x] = J.W[x];
+        if (meas && F.nchi) {
+          double* ss = reinterpret_cast<double*>(st + al16((size_t)nwords * 4));
+          for (uint32_t x = tid; x < F.nchi * J.n; x += blockDim.x) ss[x] = F.sus[x];
+          sus = ss;
+        }
+        __syncthreads();
+        S.W = Ws;
+      }
+      measure_rest(J, F, S, sus, ip, m_cur, s_cur, g);
+    }
   }
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
     J.Ec[x] = S.Ec[x];
@@ -1116,8 +1166,14 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__
     // row pointers and 16-bit column indices in shared memory for the cluster search
     uint32_t* rp = reinterpret_cast<uint32_t*>(base + o2);
     uint16_t* cl = reinterpret_cast<uint16_t*>(base + o2 + al16((size_t)(J.n + 1) * 4));
-    for (uint32_t x = threadIdx.x; x <= J.n; x += blockDim.x) rp[x] = J.F.rp[x];
-    for (uint32_t x = threadIdx.x; x < J.F.nnz; x += blockDim.x) cl[x] = (uint16_t)J.F.ent[x].x;
+    // 16-byte copies: rp (n + 1 words, tail by words) and the padded 16-bit columns
+    const uint32_t nrp4 = (J.n + 1) / 4;
+    for (uint32_t x = threadIdx.x; x < nrp4; x += blockDim.x)
+      reinterpret_cast<uint4*>(rp)[x] = reinterpret_cast<const uint4*>(J.F.rp)[x];
+    for (uint32_t x = 4 * nrp4 + threadIdx.x; x <= J.n; x += blockDim.x) rp[x] = J.F.rp[x];
+    const uint32_t ncl8 = (J.F.nnz + 7) / 8;
+    for (uint32_t x = threadIdx.x; x < ncl8; x += blockDim.x)
+      reinterpret_cast<uint4*>(cl)[x] = reinterpret_cast<const uint4*>(J.F.col16)[x];
     __syncthreads();
     F.rp = rp;
     cols = cl;
@@ -1337,11 +1393,16 @@ int fused_blocks_per_sm(uint32_t T, size_t smem) {
   return nb;
 }
 
-size_t plain_head_bytes(const PtJob& j) { return plain_head_smem(j.n, j.C, j.ntp); }
+size_t plain_head_bytes(const PtJob& j, bool stage) {
+  size_t b = plain_head_smem(j.n, j.C, j.ntp);
+  if (stage) b += al16((size_t)j.n * j.nw * 4) + al16((size_t)j.F.nchi * j.n * 8);
+  return b;
+}
 
-void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem) {
+void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem,
+                       int stage) {
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_head, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_plain_head<<<1, 1024, smem, st>>>(d_job, ctl, acc, mode);
+  k_plain_head<<<1, 1024, smem, st>>>(d_job, ctl, acc, mode, stage);
   TAMC_CUDA(cudaGetLastError());
 }
 
@@ -1356,7 +1417,7 @@ bool plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, Plain
                       uint32_t* icm_valid, size_t smem_limit, unsigned long long* dm) {
   const uint32_t nact = j.nt - j.lo, grid = (j.C / 2) * nact;
   if (!j.icm || grid == 0) return false;
-  const int stage = j.n <= 65536 && plain_icm_staged_bytes(j) <= smem_limit;
+  const int stage = j.F.col16 && plain_icm_staged_bytes(j) <= smem_limit;
   const size_t smem = std::max(stage ? plain_icm_staged_bytes(j) : plain_icm_bytes(j), plain_head_smem(j.n, j.C, j.ntp));
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_icm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_plain_icm<<<grid, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, stage, dm);

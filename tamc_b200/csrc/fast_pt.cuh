@@ -54,9 +54,11 @@ struct PlainCtl {
   uint32_t pending;  // the sweeps of round i-1 ran; their sums and measurements are pending
   uint32_t icm_done; // Houdayer CTAs of the current round that finished (reset by the last)
 };
-size_t plain_head_bytes(const PtJob& j);
+// with stage: room to hold the replica words and weights of a measured round
+size_t plain_head_bytes(const PtJob& j, bool stage);
 // mode 1: close the previous round (sweep sums, measurements); 2: set initial energies
-void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem);
+void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem,
+                       int stage);
 size_t plain_icm_bytes(const PtJob& j);
 // Houdayer moves of round ctl->i, one CTA per (chain pair, slot >= lo); the
 // last CTA also runs the exchange decisions (writing dm).  Returns false, and
