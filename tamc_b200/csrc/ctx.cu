@@ -217,6 +217,9 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
     d->d_perm = dmalloc_copy(d->h_perm.data(), d->h_perm.size());
     d->d_iperm = dmalloc_copy(iperm.data(), iperm.size());
     d->d_frp = dmalloc_copy(frp.data(), frp.size());
+    d->udeg = h.n ? frp[1] : 0;
+    for (uint32_t s = 0; s < h.n && d->udeg; ++s)
+      if (frp[s + 1] - frp[s] != d->udeg) d->udeg = 0;
     d->d_fent = dmalloc_copy(fent.data(), fent.size());
     if (h.n <= 65536) {
       std::vector<uint16_t> c16((fent.size() + 7) / 8 * 8 + 8, 0);

@@ -197,6 +197,7 @@ struct tamc_inst {
   uint32_t* d_frp = nullptr;         // n + 1
   uint2* d_fent = nullptr;           // nnz (col_new, J bits)
   uint16_t* d_fcol16 = nullptr;      // nnz col_new as 16 bits, padded to 8 entries (n <= 65536 only)
+  uint32_t udeg = 0;                 // entries per row when every row has the same count, else 0
   float* d_fbias = nullptr;          // n
   float* d_fkd = nullptr;            // n: self-loop coefficient (0 if none)
   double* d_fsus = nullptr;          // [nchi][n] colour order

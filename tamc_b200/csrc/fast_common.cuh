@@ -21,6 +21,7 @@ struct FastInst {  // colour-ordered instance (device pointers)
   const uint32_t* rp;         // n + 1
   const uint2* ent;           // nnz (new column, J bits)
   const uint16_t* col16;      // nnz new column as 16 bits, padded to 8 entries; null if n > 65536
+  uint32_t udeg;              // entries per row if uniform (row s = [s*udeg, (s+1)*udeg)), else 0
   const float* bias;          // n
   const float* kd;            // n self-loop coefficient
   const double* sus;          // [nchi][n], colour order
@@ -40,6 +41,26 @@ __device__ __forceinline__ float4 local_field4(uint32_t s, uint32_t shift, const
   float4 f = make_float4(h, h, h, h);
   for (uint32_t e = e0; e < e1; ++e) {
     const uint2 c = ent[e];
+    const uint32_t w = W[c.x * ws + wo] >> shift;
+    f.x += __uint_as_float(c.y ^ (w << 31));
+    f.y += __uint_as_float(c.y ^ ((w << 30) & 0x80000000u));
+    f.z += __uint_as_float(c.y ^ ((w << 29) & 0x80000000u));
+    f.w += __uint_as_float(c.y ^ ((w << 28) & 0x80000000u));
+  }
+  return f;
+}
+
+// The same with every row holding exactly DEG entries (row s starts at
+// s*DEG): no row-pointer loads, and the loop unrolls.  Same sums, same order.
+template <uint32_t DEG>
+__device__ __forceinline__ float4 local_field4_deg(uint32_t s, uint32_t shift, const uint2* __restrict__ ent,
+                                                   const float* __restrict__ bias, const uint32_t* W, uint32_t ws,
+                                                   uint32_t wo) {
+  const float h = bias[s];
+  float4 f = make_float4(h, h, h, h);
+#pragma unroll
+  for (uint32_t k = 0; k < DEG; ++k) {
+    const uint2 c = ent[s * DEG + k];
     const uint32_t w = W[c.x * ws + wo] >> shift;
     f.x += __uint_as_float(c.y ^ (w << 31));
     f.y += __uint_as_float(c.y ^ ((w << 30) & 0x80000000u));
@@ -85,10 +106,11 @@ struct Fx4 {
 
 // One quad update with inverse temperatures pre-scaled by log2(e).  Returns
 // the 4-bit flip mask; with ACC, adds accepted ΔE to acc in fixed point.
-template <bool ACC>
+template <bool ACC, uint32_t DEG = 0>
 __device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
                                                 uint32_t ws, uint32_t wo, float4 bl2, uint4 rnd, Fx4& acc) {
-  const float4 f = local_field4(s, shift, F.rp, F.ent, F.bias, W, ws, wo);
+  const float4 f = DEG ? local_field4_deg<DEG>(s, shift, F.ent, F.bias, W, ws, wo)
+                       : local_field4(s, shift, F.rp, F.ent, F.bias, W, ws, wo);
   const uint32_t own = W[s * ws + wo] >> shift;
   const float4 d = delta4(f, own);
   const bool a0 = accept1(d.x, bl2.x, rnd.x);

@@ -20,7 +20,7 @@ namespace tamc {
 
 namespace {
 
-template <int NQ, bool SMEM>
+template <int NQ, bool SMEM, uint32_t DEG>
 __global__ void __launch_bounds__(1024) k_sa_fast(SaFastArgs a) {
   extern __shared__ uint4 smem_u4[];
   constexpr uint32_t G = 4 * NQ;
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(1024) k_sa_fast(SaFastArgs a) {
       const uint32_t c1 = a.F.color_off[c + 1];
       for (uint32_t s = a.F.color_off[c] + tid / NQ; s < c1; s += stride) {
         const uint4 rnd = philox4x32_10(make_uint4(s, sw, qid, PTAG_SWEEP), PK);
-        const uint32_t m = quad_update<false>(s, shift, F, W, 1, 0, beta, rnd, acc);
+        const uint32_t m = quad_update<false, DEG>(s, shift, F, W, 1, 0, beta, rnd, acc);
         if (m) {
           if (NQ == 1) W[s] ^= m;
           else atomicXor(&W[s], m << shift);
@@ -133,12 +133,24 @@ __global__ void k_pack_states(const uint32_t* __restrict__ words, uint32_t n, ui
   out[x] = (uint8_t)v;
 }
 
-template <int NQ, bool SMEM>
-void launch_t(cudaStream_t st, const SaFastArgs& a, uint32_t ncta, uint32_t T, size_t smem) {
-  auto k = k_sa_fast<NQ, SMEM>;
+template <int NQ, bool SMEM, uint32_t DEG>
+void launch_d(cudaStream_t st, const SaFastArgs& a, uint32_t ncta, uint32_t T, size_t smem) {
+  auto k = k_sa_fast<NQ, SMEM, DEG>;
   TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<ncta, T, smem, st>>>(a);
   TAMC_CUDA(cudaGetLastError());
+}
+
+// rows of uniform length 3, 4 or 6 (random regular graphs, square and cubic
+// lattices) get an unrolled local field without row-pointer loads
+template <int NQ, bool SMEM>
+void launch_t(cudaStream_t st, const SaFastArgs& a, uint32_t ncta, uint32_t T, size_t smem) {
+  switch (a.F.udeg) {
+    case 3: launch_d<NQ, SMEM, 3>(st, a, ncta, T, smem); break;
+    case 4: launch_d<NQ, SMEM, 4>(st, a, ncta, T, smem); break;
+    case 6: launch_d<NQ, SMEM, 6>(st, a, ncta, T, smem); break;
+    default: launch_d<NQ, SMEM, 0>(st, a, ncta, T, smem); break;
+  }
 }
 
 }  // namespace

@@ -35,6 +35,7 @@ FastInst make_fast_inst(const tamc_inst* d) {
   F.rp = d->d_frp;
   F.ent = d->d_fent;
   F.col16 = d->d_fcol16;
+  F.udeg = d->udeg;
   F.bias = d->d_fbias;
   F.kd = d->d_fkd;
   F.sus = d->d_fsus;
