@@ -349,7 +349,7 @@ def workload_batch_c3(args, tb, gi, gpu):
     l_batch = gpu.launches - l0
     # plain form (one instance at a time, one launch per sweep phase) on a subset
     os.environ["TAMC_PT_FORM"] = "plain"
-    sub = list(range(0, 256, 16))
+    sub = list(range(0, 256, 256 // args.c3_plain)) if args.c3_plain > 0 else []
     f_sub, t_sub = 0, 0.0
     for k in sub:
         L, nt = jobs[k]
@@ -359,11 +359,11 @@ def workload_batch_c3(args, tb, gi, gpu):
         t_sub += t
         f_sub += L * L * nt * 2 * sweeps
     del os.environ["TAMC_PT_FORM"]
-    plain_rate = f_sub / t_sub
+    plain_rate = f_sub / t_sub if t_sub > 0 else None
     return {"workload": "batch_c3", "instances": 256, "sweeps": sweeps, "flips": flips,
             "batched_flips_per_s": flips / t_batch, "batched_s": t_batch, "batched_launches": int(l_batch),
             "plain_flips_per_s": plain_rate, "plain_sample": f"{len(sub)} of 256 instances",
-            "batched_over_plain": (flips / t_batch) / plain_rate}
+            "batched_over_plain": (flips / t_batch) / plain_rate if plain_rate else None}
 
 
 def workload_pt_c4(args, tb, gi, gpu):
@@ -465,6 +465,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--workload", default="sa_c2", choices=["sa_c2", "pt_c1", "batch_c3", "pt_c4", "serve_c5"])
     ap.add_argument("--c3-sweeps", type=int, default=5000)
+    ap.add_argument("--c3-plain", type=int, default=16, help="instances of the plain-form comparison (0 skips it)")
     ap.add_argument("--c4-sweeps", type=int, default=20000)
     ap.add_argument("--c4-cpu-sweeps", type=int, default=200)
     ap.add_argument("--c5-requests", type=int, default=1000)
