@@ -237,6 +237,10 @@ __device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red) {
 // only on the replica state, the seed and the sweep index -- not on the
 // algorithm, the number of threads or how slots are grouped -- and the fused
 // and plain forms agree.
+// PLAIN: the one-slot-per-CTA kernel of the plain form, which gets the
+// single-slot queue search and batched edge loads; the fused kernel keeps the
+// general paths (it runs at its register limit).
+template <bool PLAIN>
 __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScratch& X, uint32_t i, uint32_t p,
                           uint32_t w, uint32_t gmask, const uint16_t* cols = nullptr, uint32_t* wstage = nullptr,
                           PhaseClock* pc = nullptr) {
@@ -416,7 +420,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     }
     __syncthreads();
     if (pc) pc->lap(PHASE_ICM_MARK);
-  } else if (G == 1) {
+  } else if (PLAIN && G == 1) {
     // One slot: a site joins the cluster exactly once (the atomicOr that sets
     // its bit tells which thread got there first), so the levels are
     // consecutive segments of one queue V, which ends up listing the cluster.
@@ -566,7 +570,15 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
             const float h = bias[s];
             float f0 = h, f1 = h;
             const uint32_t e1 = rp[s + 1];
-            for (uint32_t e = rp[s]; e < e1; e += 8) {
+            if (!PLAIN) {
+              for (uint32_t e = rp[s]; e < e1; ++e) {
+                const uint2 ce = ent[e];
+                if (ce.x == s || ((XC[ce.x] >> b) & 1u)) continue;
+                const float Jv = __uint_as_float(ce.y);
+                f0 += ((r0(ce.x) >> b) & 1u) ? -Jv : Jv;
+                f1 += ((r1(ce.x) >> b) & 1u) ? -Jv : Jv;
+              }
+            } else for (uint32_t e = rp[s]; e < e1; e += 8) {
               // up to 8 entries loaded before use (independent loads in flight),
               // then summed in row order
               uint2 ce[8];
@@ -634,7 +646,7 @@ __device__ void icm_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i
           m &= m - 1;
         }
         lomask &= ~gmask;
-        icm_group(J, F, S.W, S.X, i, p, w, gmask, nullptr, nullptr, &pc);
+        icm_group<false>(J, F, S.W, S.X, i, p, w, gmask, nullptr, nullptr, &pc);
         __syncthreads();
         pc.lap(PHASE_ICM_APPLY);
         if (tid < 32 && ((gmask >> tid) & 1u) && S.X.cnt[tid]) {
@@ -767,6 +779,28 @@ __device__ void permute_words(const PtJob& J, Smem& S) {
   __syncthreads();
 }
 
+// The sites of colour class [c0, c1) for this thread's quad; DEG > 0 when
+// every row has DEG entries (unrolled local field, no row pointers).
+template <bool SELF, uint32_t DEG>
+__device__ __forceinline__ void sweep_class(const PtJob& J, const FastInst& F, Smem& S, uint32_t i, uint32_t c0,
+                                            uint32_t c1, uint32_t stride, uint32_t shift, uint32_t wo, uint32_t qid,
+                                            float4 beta, Fx4& acc, Fx4& qacc) {
+  for (uint32_t s = c0; s < c1; s += stride) {
+    const uint4 rnd = philox4x32_10(make_uint4(s, i, qid, PTAG_SWEEP), J.key);
+    const uint32_t m = quad_update<true, DEG>(s, shift, F, S.W, J.nw, wo, beta, rnd, acc);
+    if (m) {
+      atomicXor(&S.W[s * J.nw + wo], m << shift);
+      if (SELF) {
+        const long long k2 = to_fx(2.0f * J.F.kd[s]);
+        qacc.x += (m & 1u) ? k2 : 0;
+        qacc.y += (m & 2u) ? k2 : 0;
+        qacc.z += (m & 4u) ? k2 : 0;
+        qacc.w += (m & 8u) ? k2 : 0;
+      }
+    }
+  }
+}
+
 template <bool SELF>
 __device__ void sweep_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i, uint32_t Teff) {
   const uint32_t tid = threadIdx.x;
@@ -780,21 +814,9 @@ __device__ void sweep_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t
   Fx4 qacc{0, 0, 0, 0};
   for (uint32_t c = 0; c < F.ncolors; ++c) {
     if (tid < Teff) {
-      const uint32_t c1 = J.F.color_off[c + 1];
-      for (uint32_t s = J.F.color_off[c] + tid / J.qps; s < c1; s += stride) {
-        const uint4 rnd = philox4x32_10(make_uint4(s, i, qid, PTAG_SWEEP), J.key);
-        const uint32_t m = quad_update<true>(s, shift, F, S.W, J.nw, wo, beta, rnd, acc);
-        if (m) {
-          atomicXor(&S.W[s * J.nw + wo], m << shift);
-          if (SELF) {
-            const long long k2 = to_fx(2.0f * J.F.kd[s]);
-            qacc.x += (m & 1u) ? k2 : 0;
-            qacc.y += (m & 2u) ? k2 : 0;
-            qacc.z += (m & 4u) ? k2 : 0;
-            qacc.w += (m & 8u) ? k2 : 0;
-          }
-        }
-      }
+      const uint32_t c0 = J.F.color_off[c] + tid / J.qps, c1 = J.F.color_off[c + 1];
+      if (F.udeg == 4) sweep_class<SELF, 4>(J, F, S, i, c0, c1, stride, shift, wo, qid, beta, acc, qacc);
+      else sweep_class<SELF, 0>(J, F, S, i, c0, c1, stride, shift, wo, qid, beta, acc, qacc);
     }
     __syncthreads();
   }
@@ -1181,7 +1203,7 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__
   const uint32_t b = t & 31u;
   PhaseClock pc;  // with profiling on, cycles are summed over the CTAs
   pc.start(J.prof);
-  icm_group(J, F, J.W, X, ctl->i, p, t >> 5, 1u << b, cols, wstage, &pc);
+  icm_group<true>(J, F, J.W, X, ctl->i, p, t >> 5, 1u << b, cols, wstage, &pc);
   __syncthreads();
   if (threadIdx.x == 0) {
     const uint32_t x0 = 2 * p * J.ntp + t, x1 = (2 * p + 1) * J.ntp + t;
@@ -1281,7 +1303,7 @@ __global__ void __launch_bounds__(256) k_plain_perm(const PtJob* __restrict__ jp
 // The grid stride is a multiple of qps, so every thread keeps one quad k for
 // all its tasks and accumulates its fixed-point ΔE sums in registers; a CTA
 // combines its threads per slot and adds one 64-bit atomic per slot.
-template <bool SELF>
+template <bool SELF, uint32_t DEG>
 __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ jp, const PlainCtl* __restrict__ ctl,
                                                      uint32_t color, long long* acc) {
   extern __shared__ uint4 smem_u4[];
@@ -1312,7 +1334,7 @@ __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ j
   for (uint64_t site = s_first; site < nc; site += s_step) {
     const uint32_t s = c0 + (uint32_t)site;
     const uint4 rnd = philox4x32_10(make_uint4(s, i, ch * 16u + q, PTAG_SWEEP), key);
-    const uint32_t m = quad_update<true>(s, shift, F, W, nw, wo, bl2, rnd, a);
+    const uint32_t m = quad_update<true, DEG>(s, shift, F, W, nw, wo, bl2, rnd, a);
     if (m) {
       atomicXor(&W[s * nw + wo], m << shift);
       if (SELF) {
@@ -1449,12 +1471,19 @@ void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, con
   const uint32_t g = j.qps / std::gcd(j.qps, T);
   grid = std::max(g, (grid + g - 1) / g * g);
   const size_t smem = (size_t)T * sizeof(Fx4) + (size_t)j.qps * 16;
+  auto go = [&](auto k) {
+    TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, T, smem, st>>>(d_job, ctl, color, acc);
+  };
+  const uint32_t deg = j.F.udeg == 4 || j.F.udeg == 6 ? j.F.udeg : 0;
   if (j.self_loops) {
-    TAMC_CUDA(cudaFuncSetAttribute(k_plain_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plain_sweep<true><<<grid, T, smem, st>>>(d_job, ctl, color, acc);
+    if (deg == 4) go(k_plain_sweep<true, 4>);
+    else if (deg == 6) go(k_plain_sweep<true, 6>);
+    else go(k_plain_sweep<true, 0>);
   } else {
-    TAMC_CUDA(cudaFuncSetAttribute(k_plain_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plain_sweep<false><<<grid, T, smem, st>>>(d_job, ctl, color, acc);
+    if (deg == 4) go(k_plain_sweep<false, 4>);
+    else if (deg == 6) go(k_plain_sweep<false, 6>);
+    else go(k_plain_sweep<false, 0>);
   }
   TAMC_CUDA(cudaGetLastError());
 }
