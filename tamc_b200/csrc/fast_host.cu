@@ -60,10 +60,13 @@ static bool fits(const tamc_gpu* g, const PtJob& j, uint32_t T, bool csr) {
   return fused_smem_bytes(j, T, csr) <= g->smem_optin;
 }
 
+// 512 threads with the instance in shared memory if that fits, else the
+// largest CTA (512, 256, 128) whose shared memory fits without it.
 static TileChoice heuristic_tile(const tamc_gpu* g, const PtJob& j) {
-  TileChoice t{512, true};
-  if (!fits(g, j, t.T, true)) t.csr = false;
-  return t;
+  if (fits(g, j, 512, true)) return TileChoice{512, true};
+  for (uint32_t T : {512u, 256u, 128u})
+    if (T >= j.qps && fits(g, j, T, false)) return TileChoice{T, false};
+  return TileChoice{512, false};
 }
 
 static float time_tile(tamc_gpu* g, const PtJob& proto, TileChoice t, uint32_t rounds) {
@@ -337,7 +340,7 @@ static bool choose_plain(tamc_pt* pt) {
   const char* f = getenv("TAMC_PT_FORM");
   if (f && !strcmp(f, "plain")) return true;
   if (f && !strcmp(f, "fused")) return false;
-  if (g_no_autotune) return fused_smem_bytes(pt->fast->job, 512, false) > pt->g->smem_optin;
+  if (g_no_autotune) return fused_smem_bytes(pt->fast->job, 128, false) > pt->g->smem_optin;
   const PtJob& j = pt->fast->job;
   const bool fused_fits = fused_smem_bytes(j, 128, false) <= pt->g->smem_optin;
   const bool plain_fits = plain_head_bytes(j, false) <= pt->g->smem_optin;
@@ -551,12 +554,19 @@ struct ChunkRunner {
     const char* csr_env = getenv("TAMC_PT_CSR");
     for (auto* pt : act)
       if (T < pt->fast->job.qps) T = 512;
+    uint32_t qps_max = 0;
+    for (auto* pt : act) qps_max = std::max(qps_max, pt->fast->job.qps);
     size_t smem = 0;
-    for (auto* pt : act) {
-      PtJob& j = pt->fast->job;
-      if (csr_env && csr_env[0] == '0') j.csr_smem = 0;
-      if (fused_smem_bytes(j, T, j.csr_smem) > g->smem_optin) j.csr_smem = 0;
-      smem = std::max(smem, fused_smem_bytes(j, T, j.csr_smem));
+    for (;;) {  // the largest run decides: smaller CTAs leave more shared memory
+      smem = 0;
+      for (auto* pt : act) {
+        PtJob& j = pt->fast->job;
+        if (csr_env && csr_env[0] == '0') j.csr_smem = 0;
+        if (fused_smem_bytes(j, T, j.csr_smem) > g->smem_optin) j.csr_smem = 0;
+        smem = std::max(smem, fused_smem_bytes(j, T, j.csr_smem));
+      }
+      if (smem <= g->smem_optin || T / 2 < std::max(128u, qps_max)) break;
+      T /= 2;
     }
     if (smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "a run is too large for the fused PT kernel");
     const uint32_t na = (uint32_t)act.size();

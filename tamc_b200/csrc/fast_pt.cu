@@ -86,12 +86,20 @@ struct Smem {
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Label region: G label arrays for union-find, four site arrays for BFS.
-__host__ __device__ inline size_t icm_label_words(uint32_t n, uint32_t G, bool uf) {
-  return (size_t)(uf ? G : 4u) * n;
+// Label region (32-bit words) by cluster search:
+//   ICM_UF       G label arrays of n words;
+//   ICM_BFS      (several slots) level marks [n] u32, then two frontiers and the
+//                visited list as 16-bit site indices (n <= 65536);
+//   ICM_BFS_ONE  (one slot) the queue of visited sites [n] u32.
+enum { ICM_UF = 0, ICM_BFS = 1, ICM_BFS_ONE = 2 };
+__host__ __device__ inline size_t icm_n16(uint32_t n) { return ((size_t)n + 7) / 8 * 8; }
+__host__ __device__ inline size_t icm_label_words(uint32_t n, uint32_t G, int mode) {
+  if (mode == ICM_UF) return (size_t)G * n;
+  if (mode == ICM_BFS) return (size_t)n + 3 * icm_n16(n) / 2;
+  return n;
 }
 
-__host__ __device__ inline size_t carve_icm(IcmScratch* X, char* base, size_t o, uint32_t n, uint32_t G, bool uf) {
+__host__ __device__ inline size_t carve_icm(IcmScratch* X, char* base, size_t o, uint32_t n, uint32_t G, int mode) {
   auto take = [&](size_t bytes) {
     char* p = base ? base + o : nullptr;
     o = al16(o + bytes);
@@ -99,7 +107,7 @@ __host__ __device__ inline size_t carve_icm(IcmScratch* X, char* base, size_t o,
   };
   char* D = take((size_t)n * 4);
   char* Cl = take((size_t)n * 4);
-  char* L = take(icm_label_words(n, G, uf) * 4);
+  char* L = take(icm_label_words(n, G, mode) * 4);
   char* cnt = take(32 * 4);
   char* seed = take(32 * 4);
   char* gidx = take(32 * 4);
@@ -133,7 +141,7 @@ __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uin
   };
   char* W = take((size_t)n * nw * 4);
   IcmScratch X;
-  o = carve_icm(&X, base, o, n, G, uf);
+  o = carve_icm(&X, base, o, n, G, uf ? ICM_UF : ICM_BFS);
   char* Ec = take((size_t)C * ntp * 8);
   char* Er = take((size_t)C * ntp * 8);
   char* b4 = take((size_t)qps * 16);
@@ -267,7 +275,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     }
     XD[s] = (v0 ^ v1) & gmask;
     XC[s] = 0;
-    if (!uf) XL[3 * n + s] = 0;  // BFS level marks
+    if (!uf && !PLAIN) XL[s] = 0;  // level marks of the multi-slot search (ICM_BFS layout)
   }
   if (tid < 4) X.q[tid] = 0;
   if (tid < 32) {
@@ -338,7 +346,10 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
   __syncthreads();
   if (pc) pc->lap(PHASE_ICM_SCAN);
   auto col = [&](uint32_t e) -> uint32_t { return cols ? cols[e] : ent[e].x; };
-  const uint32_t* vlist = nullptr;  // BFS: the cluster sites; union-find: all sites
+  // BFS: the cluster sites (16-bit list for several slots, 32-bit for one);
+  // union-find: all sites
+  const uint16_t* vlist16 = nullptr;
+  const uint32_t* vlist = nullptr;
   if (uf) {
     // union-find labelling of the q<0 subgraph of every slot of the group:
     // (1) every site starts as a child of its smallest lower-index neighbour in
@@ -481,15 +492,15 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     // entries so that one barrier per level separates reading, filling and
     // clearing them.  A level runs only if the previous one added a (site,
     // slot) pair, so the levels end within 32 n.
-    uint32_t* const F0 = XL;
-    uint32_t* const F1 = XL + n;
-    uint32_t* const V = XL + 2 * n;
-    uint32_t* const MK = XL + 3 * n;
+    uint32_t* const MK = XL;
+    uint16_t* const F0 = reinterpret_cast<uint16_t*>(XL + n);
+    uint16_t* const F1 = F0 + icm_n16(n);
+    uint16_t* const V = F1 + icm_n16(n);
     if (tid < 32 && ((gmask >> tid) & 1u) && X.cnt[tid]) {
       const uint32_t s0 = X.seed[tid];
       const uint32_t old = atomicOr(&XC[s0], 1u << tid);
-      if (old == 0) V[atomicAdd(&X.q[3], 1u)] = s0;
-      if (atomicMax(&MK[s0], 1u) < 1u) F0[atomicAdd(&X.q[0], 1u)] = s0;
+      if (old == 0) V[atomicAdd(&X.q[3], 1u)] = (uint16_t)s0;
+      if (atomicMax(&MK[s0], 1u) < 1u) F0[atomicAdd(&X.q[0], 1u)] = (uint16_t)s0;
     }
     __syncthreads();
     // Each frontier site is expanded by a team of BFS_LANES lanes (one edge
@@ -500,8 +511,8 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     for (uint32_t lvl = 0; lvl < 32u * n + 2u; ++lvl) {
       const uint32_t ncur = X.q[lvl % 3u];
       if (ncur == 0) break;
-      const uint32_t* cur = (lvl & 1u) ? F1 : F0;
-      uint32_t* nxt = (lvl & 1u) ? F0 : F1;
+      const uint16_t* cur = (lvl & 1u) ? F1 : F0;
+      uint16_t* nxt = (lvl & 1u) ? F0 : F1;
       uint32_t* qn = &X.q[(lvl + 1u) % 3u];
       const uint32_t mark = lvl + 2u;
       const uint32_t items = ncur * BFS_LANES;
@@ -537,14 +548,14 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
           }
           oq = __shfl_sync(0xffffffffu, oq, 0);
           ov = __shfl_sync(0xffffffffu, ov, 0);
-          if (pq) nxt[oq + __popc(bq & lt)] = j;
-          if (pv) V[ov + __popc(bv & lt)] = j;
+          if (pq) nxt[oq + __popc(bq & lt)] = (uint16_t)j;
+          if (pv) V[ov + __popc(bv & lt)] = (uint16_t)j;
         }
       }
       if (tid == 0) X.q[(lvl + 2u) % 3u] = 0;
       __syncthreads();
     }
-    vlist = V;
+    vlist16 = V;
     if (pc) pc->lap(PHASE_ICM_GROW);
   }
   const uint32_t nlist = uf ? n : X.q[3];
@@ -565,7 +576,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
         b = __fns(gmask, 0, (int)g + 1);
         if (X.cnt[b]) {
           for (uint32_t x = tw * 32 + lane; x < nlist; x += team * 32) {
-            const uint32_t s = vlist ? vlist[x] : x;
+            const uint32_t s = vlist ? vlist[x] : vlist16 ? (uint32_t)vlist16[x] : x;
             if (!((XC[s] >> b) & 1u)) continue;
             const float h = bias[s];
             float f0 = h, f1 = h;
@@ -618,7 +629,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     }
   }
   for (uint32_t x = tid; x < nlist; x += T) {
-    const uint32_t s = vlist ? vlist[x] : x;
+    const uint32_t s = vlist ? vlist[x] : vlist16 ? (uint32_t)vlist16[x] : x;
     const uint32_t c = XC[s];
     if (c) {
       atomicXor(&W[s * nw + o0], c);
@@ -1170,7 +1181,7 @@ __device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long lo
 
 // Houdayer moves of round ctl->i: one CTA per (chain pair, slot >= lo).
 __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__ jp, PlainCtl* ctl, long long* icm_dE,
-                                                       uint32_t* icm_valid, int stage_adj, unsigned long long* dm) {
+                                                       uint32_t* icm_valid, int stage, unsigned long long* dm) {
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -1179,12 +1190,13 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__
   const uint32_t p = blockIdx.x / nact, t = J.lo + blockIdx.x % nact;
   char* base = reinterpret_cast<char*>(smem_u4);
   IcmScratch X;
-  const size_t o = carve_icm(&X, base, 0, J.n, 1, J.icm_uf != 0);
+  const size_t o = carve_icm(&X, base, 0, J.n, 1, J.icm_uf ? ICM_UF : ICM_BFS_ONE);
   FastInst F = J.F;
   const uint16_t* cols = nullptr;
-  uint32_t* wstage = reinterpret_cast<uint32_t*>(base + o);  // [2][n] the pair's replica words
-  const size_t o2 = o + al16((size_t)2 * J.n * 4);
-  if (stage_adj) {
+  // stage bit 1: the pair's replica words [2][n]; bit 0: row pointers and columns
+  uint32_t* wstage = (stage & 2) ? reinterpret_cast<uint32_t*>(base + o) : nullptr;
+  const size_t o2 = o + ((stage & 2) ? al16((size_t)2 * J.n * 4) : 0);
+  if (stage & 1) {
     // row pointers and 16-bit column indices in shared memory for the cluster search
     uint32_t* rp = reinterpret_cast<uint32_t*>(base + o2);
     uint16_t* cl = reinterpret_cast<uint16_t*>(base + o2 + al16((size_t)(J.n + 1) * 4));
@@ -1405,6 +1417,7 @@ __global__ void k_plain_energy(const PtJob* __restrict__ jp, long long* acc) {
 }  // namespace
 
 size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem) {
+  if (!j.icm_uf && j.n > 65536) return SIZE_MAX;  // the multi-slot search keeps 16-bit site lists
   return carve_all(nullptr, nullptr, j.n, j.nw, j.C, j.ntp, j.qps, T, j.F.nnz, csr_smem, j.icm_group, j.icm_uf != 0);
 }
 
@@ -1428,19 +1441,25 @@ void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long 
   TAMC_CUDA(cudaGetLastError());
 }
 
-size_t plain_icm_bytes(const PtJob& j) {
-  return carve_icm(nullptr, nullptr, 0, j.n, 1, j.icm_uf != 0) + al16((size_t)2 * j.n * 4);
+// Shared memory of the plain Houdayer kernel with the given staging (bit 0:
+// adjacency, bit 1: replica words); at least the exchange's.
+static size_t plain_icm_smem(const PtJob& j, int stage) {
+  size_t b = carve_icm(nullptr, nullptr, 0, j.n, 1, j.icm_uf ? ICM_UF : ICM_BFS_ONE);
+  if (stage & 2) b += al16((size_t)2 * j.n * 4);
+  if (stage & 1) b += al16((size_t)(j.n + 1) * 4) + al16((size_t)j.F.nnz * 2);
+  return std::max(b, plain_head_smem(j.n, j.C, j.ntp));
 }
-static size_t plain_icm_staged_bytes(const PtJob& j) {
-  return plain_icm_bytes(j) + al16((size_t)(j.n + 1) * 4) + al16((size_t)j.F.nnz * 2);
-}
+size_t plain_icm_bytes(const PtJob& j) { return plain_icm_smem(j, 0); }
 
 bool plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, long long* icm_dE,
                       uint32_t* icm_valid, size_t smem_limit, unsigned long long* dm) {
   const uint32_t nact = j.nt - j.lo, grid = (j.C / 2) * nact;
   if (!j.icm || grid == 0) return false;
-  const int stage = j.F.col16 && plain_icm_staged_bytes(j) <= smem_limit;
-  const size_t smem = std::max(stage ? plain_icm_staged_bytes(j) : plain_icm_bytes(j), plain_head_smem(j.n, j.C, j.ntp));
+  // as much staging as fits: words and adjacency, words only, nothing
+  int stage = j.F.col16 ? 3 : 2;
+  if (plain_icm_smem(j, stage) > smem_limit) stage = 2;
+  if (plain_icm_smem(j, stage) > smem_limit) stage = 0;
+  const size_t smem = plain_icm_smem(j, stage);
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_icm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_plain_icm<<<grid, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, stage, dm);
   TAMC_CUDA(cudaGetLastError());

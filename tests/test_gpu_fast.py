@@ -255,6 +255,26 @@ def test_server_admission_and_target_energy(tb, gpu):
     assert e.value.code == -9
 
 
+def test_server_largest_request_size(tb, gpu):
+    """The serving workload's largest requests (QUBO, N = 8192, 32 temperatures)
+    fit the fused kernel (smaller CTAs leave room for the search scratch), and
+    the served run equals the same run alone."""
+    h = tb.HostInstance.parse(gi.qubo_er(8192, 6.0, 42), qubo=True)
+    b = tb.geometric_betas(0.2, 5.0, 32)
+    p = tb.PtParams(30, b, int(np.argmax(b >= np.float32(1.0))), 0.5, True, 2, 8)
+    srv = tb.Server(gpu, hbm_budget_bytes=1 << 30, max_active=2, chunk_sweeps=15)
+    rid = srv.submit(h, p, 5)
+    while srv.step() != (0, 0):
+        pass
+    done, best, sweeps, lat = srv.result(rid)
+    assert done and sweeps == 30
+    r = tb.PtRun(gpu.upload(h), p, 5).run().sync()
+    S1, E1 = r.state()
+    S2, E2 = srv.state(rid)
+    assert np.array_equal(S1, S2) and np.array_equal(E1, E2)
+    assert np.all(np.isfinite(E2)) and best == r.gs()[1][-1]
+
+
 @pytest.mark.parametrize("kind", ["2d_gauss", "3d_gauss_64", "qubo"])
 def test_pt_fused_and_plain_forms_identical(tb, po, gpu, monkeypatch, kind):
     """The single-CTA fused form and the all-SM plain form run the same chain."""
