@@ -167,16 +167,17 @@ void sa_pack_states(cudaStream_t st, const uint32_t* words, uint32_t n, uint32_t
   TAMC_CUDA(cudaGetLastError());
 }
 
-// Heuristic tile: the smallest replica group (quads per CTA) that still gives
-// every SM at least one CTA.
+// Heuristic tile: 256 threads and the smallest replica group (quads per CTA)
+// that gives no SM more than two CTAs.  (On 1024 restarts of a 2000-spin
+// instance: 256 CTAs of 4 restarts, measured fastest of the 12 tiles.)
 static SaTile heuristic(const tamc_gpu* g, const FastInst& F, uint32_t R) {
   SaTile t;
-  t.T = 512;
+  t.T = 256;
   t.smem_csr = sa_fast_smem(F, 8, 1024, true) <= g->smem_optin;
   t.nq = 8;
   for (uint32_t nq : {1u, 2u, 4u, 8u}) {
     const uint32_t ncta = (R + 4 * nq - 1) / (4 * nq);
-    if (ncta <= (uint32_t)g->num_sms) { t.nq = nq; break; }
+    if (ncta <= 2u * (uint32_t)g->num_sms) { t.nq = nq; break; }
   }
   t.smem = sa_fast_smem(F, t.nq, t.T, t.smem_csr);
   return t;
@@ -200,21 +201,23 @@ SaTile sa_fast_choose(tamc_gpu* g, const FastInst& F, uint32_t R) {
   SaTile best = heuristic(g, F, R);
   const char* env = getenv("TAMC_AUTOTUNE");
   if ((!env || env[0] != '0') && R >= 64) {
-    const uint32_t nb = 8;
+    // long enough that the per-sweep cost, not the start-up, decides
+    const uint32_t nb = 64;
     float* d_b = nullptr;
     float* d_e = nullptr;
     uint32_t* d_w = nullptr;
     TAMC_CUDA(cudaMalloc((void**)&d_b, nb * 4));
     TAMC_CUDA(cudaMalloc((void**)&d_e, (size_t)R * 4));
     TAMC_CUDA(cudaMalloc((void**)&d_w, (size_t)((R + 31) / 32) * F.n * 4));
-    std::vector<float> hb(nb, 1.0f);
+    std::vector<float> hb(nb);
+    for (uint32_t k = 0; k < nb; ++k) hb[k] = 0.1f + 9.9f * (float)k / (float)(nb - 1);  // an annealing ramp
     TAMC_CUDA(cudaMemcpy(d_b, hb.data(), nb * 4, cudaMemcpyHostToDevice));
     cudaEvent_t e0, e1;
     TAMC_CUDA(cudaEventCreate(&e0));
     TAMC_CUDA(cudaEventCreate(&e1));
     float best_ms = 1e30f;
     for (uint32_t nq : {1u, 2u, 4u, 8u}) {
-      for (uint32_t T : {256u, 512u, 1024u}) {
+      for (uint32_t T : {128u, 256u, 512u, 1024u}) {
         SaTile t;
         t.nq = nq;
         t.T = T;
@@ -232,15 +235,17 @@ SaTile sa_fast_choose(tamc_gpu* g, const FastInst& F, uint32_t R) {
         a.init_words = nullptr;
         a.words_out = d_w;
         a.energies_out = d_e;
-        float ms = 0.0f;
-        for (int rep = 0; rep < 2; ++rep) {
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {  // the first run warms up; keep the fastest of the rest
+          float m = 0.0f;
           TAMC_CUDA(cudaMemsetAsync(d_w, 0, (size_t)((R + 31) / 32) * F.n * 4, g->stream));
           TAMC_CUDA(cudaEventRecord(e0, g->stream));
           sa_fast_launch(g->stream, a, t);
           TAMC_CUDA(cudaEventRecord(e1, g->stream));
           g->count();
           TAMC_CUDA(cudaEventSynchronize(e1));
-          TAMC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          TAMC_CUDA(cudaEventElapsedTime(&m, e0, e1));
+          if (rep > 0) ms = std::min(ms, m);
         }
         if (ms < best_ms) {
           best_ms = ms;
@@ -260,7 +265,7 @@ SaTile sa_fast_choose(tamc_gpu* g, const FastInst& F, uint32_t R) {
   }
   if (const char* e = getenv("TAMC_SA_T")) {
     const int v = atoi(e);
-    if (v == 256 || v == 512 || v == 1024) best.T = (uint32_t)v;
+    if (v == 128 || v == 256 || v == 512 || v == 1024) best.T = (uint32_t)v;
   }
   best.smem = sa_fast_smem(F, best.nq, best.T, best.smem_csr);
   if (best.smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the fast SA kernel");
