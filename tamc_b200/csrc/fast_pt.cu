@@ -922,8 +922,8 @@ __device__ GsSnap gs_track(const PtJob& J, Smem& S, uint32_t i) {
 // The rest of a round's measurements, after gs_track: the new minimum's
 // state, and on the sampling schedule e / q / suscept (weights `sus`,
 // [nchi][n] in colour order) and packed state samples.
-__device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const double* sus, uint32_t i,
-                             uint32_t& m_cur, uint32_t& s_cur, GsSnap g) {
+__device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const double* sus, const uint32_t* iperm,
+                             uint32_t i, uint32_t& m_cur, uint32_t& s_cur, GsSnap g) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
   const uint32_t n = J.n, nt = J.nt, C = J.C;
   if (g.fresh) {
@@ -932,7 +932,7 @@ __device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const d
     for (uint32_t wd = tid; wd < nw64; wd += blockDim.x) {
       uint64_t v = 0;
       for (uint32_t x = 0; x < 64 && wd * 64 + x < n; ++x)
-        v |= (uint64_t)((S.W[F.iperm[wd * 64 + x] * J.nw + o] >> b) & 1u) << x;
+        v |= (uint64_t)((S.W[iperm[wd * 64 + x] * J.nw + o] >> b) & 1u) << x;
       J.log.words[(size_t)g.k * nw64 + wd] = v;
     }
   }
@@ -974,7 +974,7 @@ __device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const d
       const uint32_t o = c * J.wpc + (t >> 5), b = t & 31u;
       uint32_t v = 0;
       for (uint32_t bit = 0; bit < 8 && byte * 8 + bit < n; ++bit)
-        v |= ((S.W[F.iperm[byte * 8 + bit] * J.nw + o] >> b) & 1u) << bit;
+        v |= ((S.W[iperm[byte * 8 + bit] * J.nw + o] >> b) & 1u) << bit;
       J.out.samp[(((size_t)z * J.out.S + smp) * C + c) * nb + byte] = (uint8_t)v;
     }
   }
@@ -984,7 +984,7 @@ __device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const d
 __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i, uint32_t& m_cur,
                               uint32_t& s_cur) {
   const GsSnap g = gs_track(J, S, i);
-  measure_rest(J, F, S, F.sus, i, m_cur, s_cur, g);
+  measure_rest(J, F, S, F.sus, F.iperm, i, m_cur, s_cur, g);
 }
 
 // Copy of the job descriptor in shared memory: the phase functions read its
@@ -1142,24 +1142,33 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
       const bool meas = sched(J.sample, ip, J.meas_init, J.num_sweeps);
       const bool snap = sched(J.sample_states, ip, J.meas_init, J.num_sweeps);
       const double* sus = F.sus;
+      const uint32_t* iperm = F.iperm;
       if (stage && (g.fresh || meas || snap)) {
-        // the measurements gather bits of every site: read the replica words
-        // (and the weights) once into shared memory instead of from L2
+        // the measurements gather bits of every site: read the replica words,
+        // the weights and the site permutation once into shared memory
+        // instead of gathering from L2
         char* st = base + plain_head_smem(J.n, J.C, J.ntp);
         uint32_t* Ws = reinterpret_cast<uint32_t*>(st);
         const uint32_t nwords = J.n * J.nw;
         for (uint32_t x = tid; x < nwords / 4; x += blockDim.x)
           reinterpret_cast<uint4*>(Ws)[x] = reinterpret_cast<const uint4*>(J.W)[x];
         for (uint32_t x = nwords / 4 * 4 + tid; x < nwords; x += blockDim.x) Ws[x] = J.W[x];
+        st += al16((size_t)nwords * 4);
+        if (g.fresh || snap) {
+          uint32_t* ip_s = reinterpret_cast<uint32_t*>(st);
+          for (uint32_t x = tid; x < J.n; x += blockDim.x) ip_s[x] = F.iperm[x];
+          iperm = ip_s;
+        }
+        st += al16((size_t)J.n * 4);
         if (meas && F.nchi) {
-          double* ss = reinterpret_cast<double*>(st + al16((size_t)nwords * 4));
+          double* ss = reinterpret_cast<double*>(st);
           for (uint32_t x = tid; x < F.nchi * J.n; x += blockDim.x) ss[x] = F.sus[x];
           sus = ss;
         }
         __syncthreads();
         S.W = Ws;
       }
-      measure_rest(J, F, S, sus, ip, m_cur, s_cur, g);
+      measure_rest(J, F, S, sus, iperm, ip, m_cur, s_cur, g);
     }
   }
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
@@ -1430,7 +1439,7 @@ int fused_blocks_per_sm(uint32_t T, size_t smem) {
 
 size_t plain_head_bytes(const PtJob& j, bool stage) {
   size_t b = plain_head_smem(j.n, j.C, j.ntp);
-  if (stage) b += al16((size_t)j.n * j.nw * 4) + al16((size_t)j.F.nchi * j.n * 8);
+  if (stage) b += al16((size_t)j.n * j.nw * 4) + al16((size_t)j.n * 4) + al16((size_t)j.F.nchi * j.n * 8);
   return b;
 }
 
