@@ -137,7 +137,8 @@ void* tamc_gpu_stream(tamc_gpu* g);
 uint64_t tamc_gpu_launch_count(tamc_gpu* g);
 
 /* Uploads the instance: reference-order CSR, ICM graph, colour-sorted CSR for
- * the fast mode and the susceptibility weights. */
+ * the fast mode and the susceptibility weights.  An instance with no sites is
+ * refused with TAMC_E_INVAL. */
 int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* h, tamc_inst** out);
 int tamc_gpu_instance_destroy(tamc_inst* d);
 

@@ -151,6 +151,9 @@ uint64_t tamc_gpu_launch_count(tamc_gpu* g) { return g ? g->launches.load() : 0;
 int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_inst** out) {
   TAMC_API_BEGIN
   if (!g || !hi || !out) fail(TAMC_E_INVAL, "null argument");
+  // an instance without sites has nothing to sample; refused here rather than
+  // launching empty grids
+  if (hi->h.n == 0) fail(TAMC_E_INVAL, "instance has no sites");
   TAMC_CUDA(cudaSetDevice(g->device));
   const HostInstance& h = hi->h;
   auto* d = new tamc_inst();
