@@ -446,14 +446,24 @@ class PtRun:
             self.h = None
 
 
-def sa_run(dinst: DeviceInstance, betas, num_replicas: int, threads: int, seed: int, mode: int = MODE_FAST):
-    """SaRunner::run / run_parallel on the device: (energies, packed states [r_eff, ceil(n/8)])."""
+def sa_run(dinst: DeviceInstance, betas, num_replicas: int, threads: int, seed: int, mode: int = MODE_FAST,
+           out=None):
+    """SaRunner::run / run_parallel on the device: (energies, packed states [r_eff, ceil(n/8)]).
+    `out` = (energies float32[r], packed uint8[r, ceil(n/8)]) receives the results
+    in caller-owned (e.g. pinned) host buffers with room for every replica."""
     b = np.ascontiguousarray(betas, np.float32)
     parts = threads if num_replicas > 1 else 1
     per = num_replicas // threads if num_replicas > 1 and threads else 1
     rmax = max(parts * per, 1)
-    e = np.zeros(rmax, np.float32)
-    packed = np.zeros((rmax, (dinst.n + 7) // 8), np.uint8)
+    if out is None:
+        e = np.zeros(rmax, np.float32)
+        packed = np.zeros((rmax, (dinst.n + 7) // 8), np.uint8)
+    else:
+        e, packed = out
+        if (e.dtype != np.float32 or packed.dtype != np.uint8 or len(e) < rmax or packed.shape[0] < rmax
+                or packed.shape[1] != (dinst.n + 7) // 8 or not e.flags.c_contiguous
+                or not packed.flags.c_contiguous):
+            raise ValueError("out buffers must be contiguous float32[r] and uint8[r, ceil(n/8)]")
     reff = C.c_uint32()
     _check(lib().tamc_gpu_sa_run(dinst.h, _p(b, f32p), len(b), num_replicas, threads, seed, mode, _p(e, f32p),
                                  _p(packed, u8p), C.byref(reff)))

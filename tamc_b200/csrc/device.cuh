@@ -139,8 +139,9 @@ struct SaScratch {
   uint32_t* words = nullptr;
   float* energies = nullptr;
   uint8_t* packed = nullptr;
-  size_t cap_words = 0, cap_e = 0, cap_packed = 0;
-  void ensure(size_t nwords, size_t ne, size_t npacked) {
+  float* betas = nullptr;
+  size_t cap_words = 0, cap_e = 0, cap_packed = 0, cap_betas = 0;
+  void ensure(size_t nwords, size_t ne, size_t npacked, size_t nbetas) {
     auto grow = [](auto*& p, size_t& cap, size_t want, size_t elt) {
       if (want <= cap) return;
       if (p) cudaFree(p);
@@ -152,15 +153,18 @@ struct SaScratch {
     grow(words, cap_words, nwords, 4);
     grow(energies, cap_e, ne, 4);
     grow(packed, cap_packed, npacked, 1);
+    grow(betas, cap_betas, nbetas, 4);
   }
   void release() {
     if (words) cudaFree(words);
     if (energies) cudaFree(energies);
     if (packed) cudaFree(packed);
+    if (betas) cudaFree(betas);
     words = nullptr;
     energies = nullptr;
     packed = nullptr;
-    cap_words = cap_e = cap_packed = 0;
+    betas = nullptr;
+    cap_words = cap_e = cap_packed = cap_betas = 0;
   }
 };
 

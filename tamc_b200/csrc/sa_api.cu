@@ -70,6 +70,33 @@ int tamc_gpu_sa_run(tamc_inst* inst, const float* betas, uint32_t nbeta, uint32_
   if (r_eff) *r_eff = R;
   if (R == 0) return TAMC_OK;
   const uint32_t nbytes = (n + 7) / 8;
+  if (mode == TAMC_MODE_FAST) {
+    // device buffers (schedule, words, energies, packed states) are cached on
+    // the instance and reused across calls; results go straight to the caller
+    SaScratch& sc = inst->sa_scratch;
+    const uint32_t nw = (R + 31) / 32;
+    sc.ensure((size_t)nw * n, R, (size_t)R * nbytes, nbeta);
+    if (nbeta) TAMC_CUDA(cudaMemcpyAsync(sc.betas, betas, nbeta * 4, cudaMemcpyHostToDevice, st));
+    TAMC_CUDA(cudaMemsetAsync(sc.words, 0, (size_t)nw * n * 4, st));
+    SaFastArgs a;
+    a.F = make_fast_inst(inst);
+    a.betas = sc.betas;
+    a.nbeta = nbeta;
+    a.key = philox_key(seed);
+    a.R = R;
+    a.init_words = nullptr;
+    a.words_out = sc.words;
+    a.energies_out = sc.energies;
+    const SaTile t = sa_fast_choose(g, a.F, R);
+    sa_fast_launch(st, a, t);
+    sa_pack_states(st, sc.words, n, R, sc.packed);
+    g->count(2);
+    if (energies_out) TAMC_CUDA(cudaMemcpyAsync(energies_out, sc.energies, R * 4, cudaMemcpyDeviceToHost, st));
+    if (packed_out)
+      TAMC_CUDA(cudaMemcpyAsync(packed_out, sc.packed, (size_t)R * nbytes, cudaMemcpyDeviceToHost, st));
+    TAMC_CUDA(cudaStreamSynchronize(st));
+    return TAMC_OK;
+  }
   DBuf<float> d_betas(nbeta);
   if (nbeta) TAMC_CUDA(cudaMemcpyAsync(d_betas.p, betas, nbeta * 4, cudaMemcpyHostToDevice, st));
   std::vector<float> e(R);
@@ -105,30 +132,6 @@ int tamc_gpu_sa_run(tamc_inst* inst, const float* betas, uint32_t nbeta, uint32_
     for (uint32_t r = 0; r < R; ++r)
       for (uint32_t i = 0; i < n; ++i)
         if (spins[(size_t)r * n + i] <= 0) packed[(size_t)r * nbytes + i / 8] |= (uint8_t)(1u << (i % 8));
-  } else if (mode == TAMC_MODE_FAST) {
-    // device buffers are cached on the instance and reused across calls
-    SaScratch& sc = inst->sa_scratch;
-    const uint32_t nw = (R + 31) / 32;
-    sc.ensure((size_t)nw * n, R, (size_t)R * nbytes);
-    TAMC_CUDA(cudaMemsetAsync(sc.words, 0, (size_t)nw * n * 4, st));
-    SaFastArgs a;
-    a.F = make_fast_inst(inst);
-    a.betas = d_betas.p;
-    a.nbeta = nbeta;
-    a.key = philox_key(seed);
-    a.R = R;
-    a.init_words = nullptr;
-    a.words_out = sc.words;
-    a.energies_out = sc.energies;
-    const SaTile t = sa_fast_choose(g, a.F, R);
-    sa_fast_launch(st, a, t);
-    sa_pack_states(st, sc.words, n, R, sc.packed);
-    g->count(2);
-    if (energies_out) TAMC_CUDA(cudaMemcpyAsync(energies_out, sc.energies, R * 4, cudaMemcpyDeviceToHost, st));
-    if (packed_out)
-      TAMC_CUDA(cudaMemcpyAsync(packed_out, sc.packed, (size_t)R * nbytes, cudaMemcpyDeviceToHost, st));
-    TAMC_CUDA(cudaStreamSynchronize(st));
-    return TAMC_OK;
   } else {
     fail(TAMC_E_INVAL, "unknown mode");
   }
