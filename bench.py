@@ -229,6 +229,9 @@ def run_gpu(args):
     e_min = float(energies.min().item())
     # the reported quality of an anneal: best energy and the share of restarts reaching it
     frac_best = float((energies <= e_min + 1e-4 * max(1.0, abs(e_min))).float().mean().item())
+    # time to target with 99 % confidence, target = this run's best energy: one anneal
+    # of all restarts succeeds with P = 1 - (1 - frac)^restarts
+    p_anneal = 1.0 - (1.0 - frac_best) ** N_REPLICAS
 
     # end-to-end through the C ABI with host buffers
     reff = 0
@@ -267,7 +270,9 @@ def run_gpu(args):
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{kind} burst",
                             "bytes_per_flip": BYTES_PER_FLIP},
-               "clocks": clk.summary(), "best_energy": e_min, "restarts_at_best": frac_best}
+               "clocks": clk.summary(), "best_energy": e_min, "restarts_at_best": frac_best,
+               "tts99_s": per_launch_ms / 1e3 * (1.0 if p_anneal >= 0.99 else
+                                                math.log(0.01) / math.log(1.0 - p_anneal))}
         if not args.no_cpu and world == 1:
             v, desc, cores = cpu_sample(text, betas_h)
             out["cpu_baseline"] = {"value": v, "unit": "flips/s", "cores": cores, "kind": "port", "sample": desc}
@@ -300,6 +305,20 @@ def _time_run(tb, dinst, p, seed):
     return time.perf_counter() - t0, r
 
 
+def _time_to_target(tb, dinst, p, seed, target, t_sweep):
+    """Time to target: the ground-state log is kept only after the warm-up
+    (src/pt.rs:542-583), so a second run with warm-up 0 records the running
+    minimum from the first sweep; returns the first sweep whose minimum reaches
+    `target` (or None) and that many sweeps at the measured time per sweep."""
+    q = tb.PtParams(p.num_sweeps, p.betas, p.lo_beta_idx, 0.0, p.icm, p.num_replica_chains, p.threads,
+                    p.sample, p.sample_states, p.sample_limiting)
+    steps, en, _ = tb.PtRun(dinst, q, seed).run().sync().gs()
+    hit = [int(st) for st, e in zip(steps, en) if e <= target + 1e-4 * max(1.0, abs(target))]
+    if not hit:
+        return None, None
+    return hit[0], (hit[0] + 1) * t_sweep
+
+
 def workload_pt_c1(args, tb, gi, gpu):
     """2-D EA +-J, L=16, nt=32, 2 chains, ICM, 2000 sweeps, sample 32 / states 32 / limiting 2."""
     text = gi.lattice(16, 2, "pm", 0)
@@ -311,22 +330,30 @@ def workload_pt_c1(args, tb, gi, gpu):
     t0 = time.perf_counter()
     rr = tb.PtRun(d, p, 3, tb.MODE_REF).run().sync()
     t_ref = time.perf_counter() - t0
-    gs_steps = r.gs()[0]
+    best = float(r.gs()[1][-1])
     out = {"workload": "pt_c1", "flips": flips, "fast_flips_per_s": flips / t_fast, "fast_s": t_fast,
-           "best_first_sweep": int(gs_steps[-1]), "time_to_best_s": t_fast * (int(gs_steps[-1]) + 1) / 2000,
            "ref_mode_flips_per_s": flips / t_ref, "ref_mode_s": t_ref,
-           "best_energy_fast": float(r.gs()[1][-1]), "best_energy_ref_mode": float(rr.gs()[1][-1])}
+           "best_energy_fast": best, "best_energy_ref_mode": float(rr.gs()[1][-1])}
+    target = best
     if not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import pyoracle as po
         inst = po.Instance.from_text(text)
-        t0 = time.perf_counter()
-        orc = po.PtRun(inst, p.betas, 2000, 0.5, p.lo_beta_idx, True, 2, 1, sample=32, sample_states=32,
-                       sample_limiting=2, seed=3)
-        orc.run()
-        t_cpu = time.perf_counter() - t0
-        out.update(cpu_flips_per_s=flips / t_cpu, cpu_s=t_cpu, cpu_kind="oracle, threads: 1 (serial reference loop)",
-                   cpu_best_energy=float(orc.gs()[-1][1]))
+        runs = {}
+        for threads in (1, os.cpu_count() or 1):  # the reference's run (threads: 1) and run_parallel on all cores
+            t0 = time.perf_counter()
+            orc = po.PtRun(inst, p.betas, 2000, 0.5, p.lo_beta_idx, True, 2, threads, sample=32, sample_states=32,
+                           sample_limiting=2, seed=3)
+            orc.run(nthreads=threads)
+            runs[threads] = (time.perf_counter() - t0, float(orc.gs()[-1][1]))
+        t1, e1 = runs[1]
+        tn, en = runs[max(runs)]
+        out.update(cpu_flips_per_s=flips / t1, cpu_s=t1, cpu_kind="oracle, threads: 1 (serial reference loop)",
+                   cpu_best_energy=e1, cpu_allcore_flips_per_s=flips / tn, cpu_allcore_threads=max(runs),
+                   cpu_allcore_best_energy=en)
+        target = min(e1, en, best)
+    first, tts = _time_to_target(tb, d, p, 2, target, t_fast / 2000)
+    out.update(target_energy=target, target_first_sweep=first, time_to_target_s=tts)
     return out
 
 
@@ -389,11 +416,10 @@ def workload_pt_c4(args, tb, gi, gpu):
     flips = 4096 * 64 * 2 * sweeps
     _time_run(tb, d, _lattice_params(tb, 64, 64, 32, 32, 0, threads=64), 1)  # autotune + warm-up
     t_gpu, r = _time_run(tb, d, p, 2)
-    gs_steps, gs_e, _ = r.gs()
-    # time to target: wall time until the sweep at which the final best energy was first reached
+    best = float(r.gs()[1][-1])
+    first, tts = _time_to_target(tb, d, p, 2, best, t_gpu / sweeps)
     out = {"workload": "pt_c4", "sweeps": sweeps, "flips": flips, "gpu_flips_per_s": flips / t_gpu, "gpu_s": t_gpu,
-           "gpu_best_energy": float(gs_e[-1]), "best_first_sweep": int(gs_steps[-1]),
-           "time_to_best_s": t_gpu * (int(gs_steps[-1]) + 1) / sweeps}
+           "gpu_best_energy": best, "target_energy": best, "target_first_sweep": first, "time_to_target_s": tts}
     if not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import pyoracle as po
