@@ -533,8 +533,11 @@ struct ChunkRunner {
     ctr.alloc(1);
     counts.alloc(cap_jobs);
   }
-  // Advances every run in `act` by up to `chunk` rounds.
-  void run(tamc_gpu* g, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph) {
+  // Advances every run in `act` by up to `chunk` rounds.  With `balance`, a run
+  // whose rounds cost less than the costliest run's gets proportionally more
+  // rounds (up to 8x), so that every run does about the same work per launch
+  // and small runs are not held back by large ones (the serving loop).
+  void run(tamc_gpu* g, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance = false) {
     cudaStream_t st = g->stream;
     act.erase(std::remove_if(act.begin(), act.end(),
                              [](tamc_pt* p) { return p->next_sweep >= p->cfg.num_sweeps; }),
@@ -572,12 +575,19 @@ struct ChunkRunner {
     const uint32_t na = (uint32_t)act.size();
     reserve(na);
     std::vector<uint32_t> ends(na);
+    double c_max = 1.0;  // the largest cost of one round among the runs
+    for (auto* pt : act) c_max = std::max(c_max, (double)pt->fast->job.cost / std::max(1u, pt->cfg.num_sweeps));
     for (uint32_t x = 0; x < na; ++x) {
       tamc_pt* pt = act[x];
       PtJob j = pt->fast->job;
       j.init = 0;
       j.sweep_begin = pt->next_sweep;
-      ends[x] = std::min(pt->cfg.num_sweeps, pt->next_sweep + std::min(chunk, pt->out.cap));
+      uint32_t rounds = chunk;
+      if (balance) {
+        const double c_x = (double)pt->fast->job.cost / std::max(1u, pt->cfg.num_sweeps);
+        rounds = (uint32_t)std::min<double>(8.0 * chunk, chunk * std::max(1.0, c_max / std::max(c_x, 1.0)));
+      }
+      ends[x] = std::min(pt->cfg.num_sweeps, pt->next_sweep + std::min(rounds, pt->out.cap));
       j.sweep_end = ends[x];
       j.m_base = pt->m_next;
       j.s_base = pt->s_next;
@@ -626,7 +636,7 @@ struct ChunkRunner {
 };
 
 void chunk_run(ChunkRunner* r, tamc_gpu* g, std::vector<tamc_pt*>& act, uint32_t chunk) {
-  r->run(g, act, chunk, false);
+  r->run(g, act, chunk, false, true);
 }
 ChunkRunner* chunk_runner_new() { return new ChunkRunner(); }
 void chunk_runner_free(ChunkRunner* r) { delete r; }
