@@ -177,11 +177,11 @@ def run_gpu(args):
     from tamc_b200 import instances as gi
 
     world, rank, local = _dist()
+    torch.cuda.set_device(local)  # before the process group, so NCCL binds this rank's GPU
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     gpu = tb.Gpu(local)
     text = gi.sa_regular(N_SPINS, DEGREE, 0)
