@@ -264,6 +264,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
   uint32_t* const XC = X.Cl;
   uint32_t* const XL = X.L;
   const bool uf = J.icm_uf != 0;
+  const bool prop = !uf && n <= 4 * T;  // several-slot search: propagation on small instances
   // the pair's replica words, read once (kept in shared memory when W is not)
   auto r0 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[s] : W[s * nw + o0]; };
   auto r1 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[n + s] : W[s * nw + o1]; };
@@ -431,6 +432,35 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     }
     __syncthreads();
     if (pc) pc->lap(PHASE_ICM_MARK);
+  } else if (!PLAIN && prop) {
+    // Small instances (at most 4 sites per thread): in-place propagation.  Each
+    // pass, every site still missing some of its q<0 slots takes the cluster
+    // bits of its neighbours (C[s] |= D[s] & OR_j C[j]); only the site's thread
+    // writes C[s], and a neighbour's word can only have gained bits, so reading
+    // it mid-pass is safe and lets a pass advance more than one hop.  Passes end
+    // when one changes nothing (each changing pass adds a bit: at most 32 n).
+    // Whole-graph passes cost a fixed few loads per thread, where a frontier
+    // level pays a chain of shared atomics and appends.
+    if (tid < 32 && ((gmask >> tid) & 1u) && X.cnt[tid]) atomicOr(&XC[X.seed[tid]], 1u << tid);
+    __syncthreads();
+    for (uint32_t pass = 0; pass < 32u * n + 2u; ++pass) {
+      int grew = 0;
+      for (uint32_t s = tid; s < n; s += T) {
+        const uint32_t d = XD[s];
+        const uint32_t c = XC[s];
+        if ((c & d) == d) continue;
+        uint32_t nb = 0;
+        const uint32_t e1 = rp[s + 1];
+        for (uint32_t e = rp[s]; e < e1; ++e) nb |= XC[col(e)];
+        const uint32_t nc = c | (nb & d);
+        if (nc != c) {
+          XC[s] = nc;
+          grew = 1;
+        }
+      }
+      if (!__syncthreads_or(grew)) break;
+    }
+    if (pc) pc->lap(PHASE_ICM_GROW);
   } else if (PLAIN && G == 1) {
     // One slot: a site joins the cluster exactly once (the atomicOr that sets
     // its bit tells which thread got there first), so the levels are
@@ -558,7 +588,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     vlist16 = V;
     if (pc) pc->lap(PHASE_ICM_GROW);
   }
-  const uint32_t nlist = uf ? n : X.q[3];
+  const uint32_t nlist = (uf || (!PLAIN && prop)) ? n : X.q[3];
   // energy change of flipping each cluster in both replicas: boundary terms
   // -2 s_i (h_i + sum_{j not in cluster} J_ij s_j), f32 per site, summed in
   // fixed point per slot.  The slots are dealt to teams of warps (all warps
