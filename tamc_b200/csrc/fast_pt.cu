@@ -245,6 +245,8 @@ __device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red) {
 // only on the replica state, the seed and the sweep index -- not on the
 // algorithm, the number of threads or how slots are grouped -- and the fused
 // and plain forms agree.
+// Instances of at most 4 sites per thread use in-place propagation instead of
+// a BFS (whole-graph passes, no frontier lists).
 // PLAIN: the one-slot-per-CTA kernel of the plain form, which gets the
 // single-slot queue search and batched edge loads; the fused kernel keeps the
 // general paths (it runs at its register limit).
@@ -264,7 +266,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
   uint32_t* const XC = X.Cl;
   uint32_t* const XL = X.L;
   const bool uf = J.icm_uf != 0;
-  const bool prop = !uf && n <= 4 * T;  // several-slot search: propagation on small instances
+  const bool prop = !uf && n <= 4 * T;  // propagation instead of BFS on small instances
   // the pair's replica words, read once (kept in shared memory when W is not)
   auto r0 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[s] : W[s * nw + o0]; };
   auto r1 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[n + s] : W[s * nw + o1]; };
@@ -432,7 +434,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     }
     __syncthreads();
     if (pc) pc->lap(PHASE_ICM_MARK);
-  } else if (!PLAIN && prop) {
+  } else if (prop) {
     // Small instances (at most 4 sites per thread): in-place propagation.  Each
     // pass, every site still missing some of its q<0 slots takes the cluster
     // bits of its neighbours (C[s] |= D[s] & OR_j C[j]); only the site's thread
@@ -588,7 +590,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     vlist16 = V;
     if (pc) pc->lap(PHASE_ICM_GROW);
   }
-  const uint32_t nlist = (uf || (!PLAIN && prop)) ? n : X.q[3];
+  const uint32_t nlist = (uf || prop) ? n : X.q[3];
   // energy change of flipping each cluster in both replicas: boundary terms
   // -2 s_i (h_i + sum_{j not in cluster} J_ij s_j), f32 per site, summed in
   // fixed point per slot.  The slots are dealt to teams of warps (all warps
