@@ -70,27 +70,30 @@ __device__ __forceinline__ float4 local_field4_deg(uint32_t s, uint32_t shift, c
   return f;
 }
 
-// ΔE_r = -2 s_r f_r for the quad (src/ising.rs:476-477).
-__device__ __forceinline__ float4 delta4(float4 f, uint32_t own) {
-  float4 d;
-  d.x = __uint_as_float(__float_as_uint(-2.0f * f.x) ^ (own << 31));
-  d.y = __uint_as_float(__float_as_uint(-2.0f * f.y) ^ ((own << 30) & 0x80000000u));
-  d.z = __uint_as_float(__float_as_uint(-2.0f * f.z) ^ ((own << 29) & 0x80000000u));
-  d.w = __uint_as_float(__float_as_uint(-2.0f * f.w) ^ ((own << 28) & 0x80000000u));
-  return d;
+// g_r = s_r f_r for the quad; the flip costs ΔE_r = -2 g_r (src/ising.rs:476-477).
+__device__ __forceinline__ float4 spin_field4(float4 f, uint32_t own) {
+  float4 g;
+  g.x = __uint_as_float(__float_as_uint(f.x) ^ (own << 31));
+  g.y = __uint_as_float(__float_as_uint(f.y) ^ ((own << 30) & 0x80000000u));
+  g.z = __uint_as_float(__float_as_uint(f.z) ^ ((own << 29) & 0x80000000u));
+  g.w = __uint_as_float(__float_as_uint(f.w) ^ ((own << 28) & 0x80000000u));
+  return g;
 }
 
-// Metropolis rule: accept iff u < 2^(-beta*log2(e) * max(ΔE, 0)); ΔE <= 0
-// always accepts (p = 1), as the reference's rule does.  `bl2` is beta*log2(e);
-// u is a 23-bit uniform built by placing the random mantissa under the
-// exponent of 1.0 (u + 1 in [1, 2)), compared with p + 1.
+// Metropolis rule: accept iff u < min(1, e^(-beta ΔE)) = min(1, 2^(b2 g)) with
+// b2 = 2 beta log2(e) (TAMC_2LOG2E) and g = -ΔE/2.  u is a 23-bit uniform
+// built by placing the random mantissa under the exponent of 1.0 (u + 1 in
+// [1, 2)) and compared with p + 1.  ΔE <= 0 gives p + 1 >= 2 > u + 1, so it
+// always accepts, as the reference's rule does, with no clamp.  b2 g is the
+// same float as -(beta log2 e) ΔE: both are one rounding of the same product.
+#define TAMC_2LOG2E 2.8853900817779268f
 __device__ __forceinline__ float ex2_approx(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-__device__ __forceinline__ bool accept1(float dE, float bl2, uint32_t r) {
-  const float p1 = ex2_approx(-bl2 * fmaxf(dE, 0.0f)) + 1.0f;
+__device__ __forceinline__ bool accept_g(float g, float b2, uint32_t r) {
+  const float p1 = ex2_approx(b2 * g) + 1.0f;
   return __uint_as_float(0x3f800000u | (r >> 9)) < p1;
 }
 
@@ -104,24 +107,25 @@ struct Fx4 {
   long long x, y, z, w;
 };
 
-// One quad update with inverse temperatures pre-scaled by log2(e).  Returns
-// the 4-bit flip mask; with ACC, adds accepted ΔE to acc in fixed point.
+// One quad update with inverse temperatures pre-scaled by 2 log2(e)
+// (TAMC_2LOG2E).  Returns the 4-bit flip mask; with ACC, adds accepted ΔE to
+// acc in fixed point.
 template <bool ACC, uint32_t DEG = 0>
 __device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
-                                                uint32_t ws, uint32_t wo, float4 bl2, uint4 rnd, Fx4& acc) {
+                                                uint32_t ws, uint32_t wo, float4 b2, uint4 rnd, Fx4& acc) {
   const float4 f = DEG ? local_field4_deg<DEG>(s, shift, F.ent, F.bias, W, ws, wo)
                        : local_field4(s, shift, F.rp, F.ent, F.bias, W, ws, wo);
   const uint32_t own = W[s * ws + wo] >> shift;
-  const float4 d = delta4(f, own);
-  const bool a0 = accept1(d.x, bl2.x, rnd.x);
-  const bool a1 = accept1(d.y, bl2.y, rnd.y);
-  const bool a2 = accept1(d.z, bl2.z, rnd.z);
-  const bool a3 = accept1(d.w, bl2.w, rnd.w);
+  const float4 g = spin_field4(f, own);
+  const bool a0 = accept_g(g.x, b2.x, rnd.x);
+  const bool a1 = accept_g(g.y, b2.y, rnd.y);
+  const bool a2 = accept_g(g.z, b2.z, rnd.z);
+  const bool a3 = accept_g(g.w, b2.w, rnd.w);
   if (ACC) {
-    acc.x += to_fx(a0 ? d.x : 0.0f);
-    acc.y += to_fx(a1 ? d.y : 0.0f);
-    acc.z += to_fx(a2 ? d.z : 0.0f);
-    acc.w += to_fx(a3 ? d.w : 0.0f);
+    acc.x += to_fx(a0 ? -2.0f * g.x : 0.0f);
+    acc.y += to_fx(a1 ? -2.0f * g.y : 0.0f);
+    acc.z += to_fx(a2 ? -2.0f * g.z : 0.0f);
+    acc.w += to_fx(a3 ? -2.0f * g.w : 0.0f);
   }
   return (uint32_t)a0 | ((uint32_t)a1 << 1) | ((uint32_t)a2 << 2) | ((uint32_t)a3 << 3);
 }

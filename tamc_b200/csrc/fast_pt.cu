@@ -1048,7 +1048,7 @@ __device__ void run_job(const PtJob& J, char* smem_base) {
   }
   for (uint32_t k = tid; k < J.qps; k += T) {
     const uint32_t q = k % J.qpc;
-    const float L2E = 1.4426950408889634f;  // beta * log2(e) for ex2
+    const float L2E = TAMC_2LOG2E;  // 2 beta log2(e) for ex2
     S.beta4[k] = make_float4(J.betas[4 * q] * L2E, J.betas[4 * q + 1] * L2E, J.betas[4 * q + 2] * L2E,
                              J.betas[4 * q + 3] * L2E);
   }
@@ -1363,7 +1363,7 @@ __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ j
   const PtJob& J = *jp;
   Fx4* red = reinterpret_cast<Fx4*>(smem_u4);                 // [blockDim.x]
   float4* b4 = reinterpret_cast<float4*>(red + blockDim.x);   // [qps]
-  const float L2E = 1.4426950408889634f;
+  const float L2E = TAMC_2LOG2E;
   for (uint32_t k = threadIdx.x; k < J.qps; k += blockDim.x) {
     const uint32_t q = k % J.qpc;
     b4[k] = make_float4(J.betas[4 * q] * L2E, J.betas[4 * q + 1] * L2E, J.betas[4 * q + 2] * L2E,
@@ -1377,7 +1377,7 @@ __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ j
   const uint32_t k = (uint32_t)(gtid % J.qps);
   const uint32_t ch = k / J.qpc, q = k % J.qpc;
   const uint32_t wo = ch * J.wpc + (q >> 3), shift = 4 * (q & 7u);
-  const float4 bl2 = b4[k];
+  const float4 b2 = b4[k];
   const FastInst F = J.F;
   const uint2 key = J.key;
   uint32_t* const W = J.W;
@@ -1387,7 +1387,7 @@ __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ j
   for (uint64_t site = s_first; site < nc; site += s_step) {
     const uint32_t s = c0 + (uint32_t)site;
     const uint4 rnd = philox4x32_10(make_uint4(s, i, ch * 16u + q, PTAG_SWEEP), key);
-    const uint32_t m = quad_update<true, DEG>(s, shift, F, W, nw, wo, bl2, rnd, a);
+    const uint32_t m = quad_update<true, DEG>(s, shift, F, W, nw, wo, b2, rnd, a);
     if (m) {
       atomicXor(&W[s * nw + wo], m << shift);
       if (SELF) {

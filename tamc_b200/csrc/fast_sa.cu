@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(1024) k_sa_fast(SaFastArgs a) {
   Fx4 acc{0, 0, 0, 0};  // unused: SA energies are computed once at the end
   const PhiloxKeys PK = philox_schedule(key);
   for (uint32_t sw = 0; sw < a.nbeta; ++sw) {
-    const float b = a.betas[sw] * 1.4426950408889634f;  // beta * log2(e)
+    const float b = a.betas[sw] * TAMC_2LOG2E;  // 2 beta log2(e)
     const float4 beta = make_float4(b, b, b, b);
     for (uint32_t c = 0; c < F.ncolors; ++c) {
       const uint32_t c1 = a.F.color_off[c + 1];
