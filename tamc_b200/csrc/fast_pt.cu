@@ -267,15 +267,12 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
   uint32_t* const XL = X.L;
   const bool uf = J.icm_uf != 0;
   const bool prop = !uf && n <= 4 * T;  // propagation instead of BFS on small instances
-  // the pair's replica words, read once (kept in shared memory when W is not)
+  // replica 0's words, read once (kept in shared memory when W is not); the
+  // energy change needs no other replica words
   auto r0 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[s] : W[s * nw + o0]; };
-  auto r1 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[n + s] : W[s * nw + o1]; };
   for (uint32_t s = tid; s < n; s += T) {
     const uint32_t v0 = W[s * nw + o0], v1 = W[s * nw + o1];
-    if (wstage) {
-      wstage[s] = v0;
-      wstage[n + s] = v1;
-    }
+    if (wstage) wstage[s] = v0;
     XD[s] = (v0 ^ v1) & gmask;
     XC[s] = 0;
     if (!uf && !PLAIN) XL[s] = 0;  // level marks of the multi-slot search (ICM_BFS layout)
@@ -596,6 +593,12 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
   // fixed point per slot.  The slots are dealt to teams of warps (all warps
   // for one slot, one warp per slot for many); each warp reduces by shuffles
   // and a team combines its warps in a fixed order.
+  // Only replica 0's sum is formed: the cluster is the whole component of the
+  // seed among the sites where the replicas differ, so every neighbour j
+  // outside it has the same spin in both replicas while every cluster site
+  // has opposite spins.  Replica 1's field at i is therefore the same float
+  // sum in the same order and its term is the exact negative (conversion to
+  // fixed point rounds symmetrically), so its sum is -a0, bit for bit.
   {
     const uint32_t team = max(1u, nwarp / G), teams = nwarp / team;
     const uint32_t tw = warp % team, tid_team = warp / team;
@@ -610,8 +613,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
           for (uint32_t x = tw * 32 + lane; x < nlist; x += team * 32) {
             const uint32_t s = vlist ? vlist[x] : vlist16 ? (uint32_t)vlist16[x] : x;
             if (!((XC[s] >> b) & 1u)) continue;
-            const float h = bias[s];
-            float f0 = h, f1 = h;
+            float f0 = bias[s];
             const uint32_t e1 = rp[s + 1];
             if (!PLAIN) {
               for (uint32_t e = rp[s]; e < e1; ++e) {
@@ -619,7 +621,6 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
                 if (ce.x == s || ((XC[ce.x] >> b) & 1u)) continue;
                 const float Jv = __uint_as_float(ce.y);
                 f0 += ((r0(ce.x) >> b) & 1u) ? -Jv : Jv;
-                f1 += ((r1(ce.x) >> b) & 1u) ? -Jv : Jv;
               }
             } else for (uint32_t e = rp[s]; e < e1; e += 8) {
               // up to 8 entries loaded before use (independent loads in flight),
@@ -633,14 +634,12 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
                 if (e + k >= e1 || ce[k].x == s || ((XC[ce[k].x] >> b) & 1u)) continue;
                 const float Jv = __uint_as_float(ce[k].y);
                 f0 += ((r0(ce[k].x) >> b) & 1u) ? -Jv : Jv;
-                f1 += ((r1(ce[k].x) >> b) & 1u) ? -Jv : Jv;
               }
             }
             const float s0 = ((r0(s) >> b) & 1u) ? -1.0f : 1.0f;
-            const float s1 = ((r1(s) >> b) & 1u) ? -1.0f : 1.0f;
             a0 += to_fx(-2.0f * s0 * f0);
-            a1 += to_fx(-2.0f * s1 * f1);
           }
+          a1 = -a0;
         }
       }
       for (int off = 16; off > 0; off >>= 1) {
@@ -1234,9 +1233,9 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__
   const size_t o = carve_icm(&X, base, 0, J.n, 1, J.icm_uf ? ICM_UF : ICM_BFS_ONE);
   FastInst F = J.F;
   const uint16_t* cols = nullptr;
-  // stage bit 1: the pair's replica words [2][n]; bit 0: row pointers and columns
+  // stage bit 1: replica 0's words [n]; bit 0: row pointers and columns
   uint32_t* wstage = (stage & 2) ? reinterpret_cast<uint32_t*>(base + o) : nullptr;
-  const size_t o2 = o + ((stage & 2) ? al16((size_t)2 * J.n * 4) : 0);
+  const size_t o2 = o + ((stage & 2) ? al16((size_t)J.n * 4) : 0);
   if (stage & 1) {
     // row pointers and 16-bit column indices in shared memory for the cluster search
     uint32_t* rp = reinterpret_cast<uint32_t*>(base + o2);
@@ -1486,7 +1485,7 @@ void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long 
 // adjacency, bit 1: replica words); at least the exchange's.
 static size_t plain_icm_smem(const PtJob& j, int stage) {
   size_t b = carve_icm(nullptr, nullptr, 0, j.n, 1, j.icm_uf ? ICM_UF : ICM_BFS_ONE);
-  if (stage & 2) b += al16((size_t)2 * j.n * 4);
+  if (stage & 2) b += al16((size_t)j.n * 4);
   if (stage & 1) b += al16((size_t)(j.n + 1) * 4) + al16((size_t)j.F.nnz * 2);
   return std::max(b, plain_head_smem(j.n, j.C, j.ntp));
 }
