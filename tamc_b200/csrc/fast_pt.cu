@@ -615,25 +615,52 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
             if (!((XC[s] >> b) & 1u)) continue;
             float f0 = bias[s];
             const uint32_t e1 = rp[s + 1];
-            if (!PLAIN) {
+            if (!PLAIN && F.udeg == 4) {
+              // square-lattice rows: all four entries, cluster words and spins
+              // loaded before use, then summed in row order
+              uint2 ce[4];
+              uint32_t xc[4], wv[4];
+#pragma unroll
+              for (uint32_t k = 0; k < 4; ++k) ce[k] = ent[4 * s + k];
+#pragma unroll
+              for (uint32_t k = 0; k < 4; ++k) {
+                xc[k] = XC[ce[k].x];
+                wv[k] = r0(ce[k].x);
+              }
+#pragma unroll
+              for (uint32_t k = 0; k < 4; ++k) {
+                if (ce[k].x == s || ((xc[k] >> b) & 1u)) continue;
+                const float Jv = __uint_as_float(ce[k].y);
+                f0 += ((wv[k] >> b) & 1u) ? -Jv : Jv;
+              }
+            } else if (!PLAIN) {
+              // other rows: one entry at a time (the fused kernel has no
+              // registers for batched loads)
               for (uint32_t e = rp[s]; e < e1; ++e) {
                 const uint2 ce = ent[e];
                 if (ce.x == s || ((XC[ce.x] >> b) & 1u)) continue;
                 const float Jv = __uint_as_float(ce.y);
                 f0 += ((r0(ce.x) >> b) & 1u) ? -Jv : Jv;
               }
-            } else for (uint32_t e = rp[s]; e < e1; e += 8) {
-              // up to 8 entries loaded before use (independent loads in flight),
-              // then summed in row order
-              uint2 ce[8];
+            } else for (uint32_t e = rp[s]; e < e1; e += 4) {
+              // up to 4 entries, their cluster words and spins loaded before
+              // use (independent loads in flight), then summed in row order
+              uint2 ce[4];
+              uint32_t xc[4], wv[4];
 #pragma unroll
-              for (uint32_t k = 0; k < 8; ++k)
+              for (uint32_t k = 0; k < 4; ++k)
                 if (e + k < e1) ce[k] = ent[e + k];
 #pragma unroll
-              for (uint32_t k = 0; k < 8; ++k) {
-                if (e + k >= e1 || ce[k].x == s || ((XC[ce[k].x] >> b) & 1u)) continue;
+              for (uint32_t k = 0; k < 4; ++k)
+                if (e + k < e1) {
+                  xc[k] = XC[ce[k].x];
+                  wv[k] = r0(ce[k].x);
+                }
+#pragma unroll
+              for (uint32_t k = 0; k < 4; ++k) {
+                if (e + k >= e1 || ce[k].x == s || ((xc[k] >> b) & 1u)) continue;
                 const float Jv = __uint_as_float(ce[k].y);
-                f0 += ((r0(ce[k].x) >> b) & 1u) ? -Jv : Jv;
+                f0 += ((wv[k] >> b) & 1u) ? -Jv : Jv;
               }
             }
             const float s0 = ((r0(s) >> b) & 1u) ? -1.0f : 1.0f;
