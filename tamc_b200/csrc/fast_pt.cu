@@ -250,6 +250,18 @@ __device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red) {
 // PLAIN: the one-slot-per-CTA kernel of the plain form, which gets the
 // single-slot queue search and batched edge loads; the fused kernel keeps the
 // general paths (it runs at its register limit).
+// OR of the cluster words of the DEG neighbours of s (rows of DEG entries).
+template <uint32_t DEG, typename Col>
+__device__ __forceinline__ uint32_t nb_or(uint32_t s, const uint32_t* XC, Col col) {
+  uint32_t j[DEG];
+#pragma unroll
+  for (uint32_t k = 0; k < DEG; ++k) j[k] = col(DEG * s + k);
+  uint32_t nb = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < DEG; ++k) nb |= XC[j[k]];
+  return nb;
+}
+
 template <bool PLAIN>
 __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScratch& X, uint32_t i, uint32_t p,
                           uint32_t w, uint32_t gmask, const uint16_t* cols = nullptr, uint32_t* wstage = nullptr,
@@ -442,6 +454,9 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     // level pays a chain of shared atomics and appends.
     if (tid < 32 && ((gmask >> tid) & 1u) && X.cnt[tid]) atomicOr(&XC[X.seed[tid]], 1u << tid);
     __syncthreads();
+    // rows of 4 or 6 entries (square and cubic lattices): the columns, then
+    // the neighbours' words, all loaded before use
+    const uint32_t udeg = F.udeg;
     for (uint32_t pass = 0; pass < 32u * n + 2u; ++pass) {
       int grew = 0;
       for (uint32_t s = tid; s < n; s += T) {
@@ -449,8 +464,14 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
         const uint32_t c = XC[s];
         if ((c & d) == d) continue;
         uint32_t nb = 0;
-        const uint32_t e1 = rp[s + 1];
-        for (uint32_t e = rp[s]; e < e1; ++e) nb |= XC[col(e)];
+        if (udeg == 4) {
+          nb = nb_or<4>(s, XC, col);
+        } else if (udeg == 6) {
+          nb = nb_or<6>(s, XC, col);
+        } else {
+          const uint32_t e1 = rp[s + 1];
+          for (uint32_t e = rp[s]; e < e1; ++e) nb |= XC[col(e)];
+        }
         const uint32_t nc = c | (nb & d);
         if (nc != c) {
           XC[s] = nc;
