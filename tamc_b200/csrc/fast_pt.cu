@@ -60,7 +60,8 @@ __device__ __forceinline__ float u24(uint32_t r) { return (float)(r >> 8) * (1.0
 struct IcmScratch {
   uint32_t* D;     // [n] disagreement bits of the group's slots
   uint32_t* Cl;    // [n] cluster bits
-  uint32_t* L;     // union-find: [G][n] labels; BFS: [4][n] two frontiers, visited list, level marks
+  uint32_t* L;     // union-find: [G][n] labels; several-slot BFS: [n] level marks, then two frontiers
+                   // and the visited list as 16-bit site lists; one-slot BFS: [n] queue; propagation: unused
   uint32_t* cnt;   // [32] q<0 counts per bit
   uint32_t* seed;  // [32] seed site per bit
   uint32_t* gidx;  // [32] label-array index per bit
