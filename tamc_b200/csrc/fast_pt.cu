@@ -1072,21 +1072,46 @@ __device__ GsSnap gs_track(const PtJob& J, Smem& S, uint32_t i) {
   return s_g;
 }
 
+// 32x32 bit transpose across a warp: lane L passes row L (bit c = column c)
+// and gets column L (bit r = row r's bit L).  Five butterfly steps; at step j
+// the lanes L and L^j swap the off-diagonal j x j blocks of their 2j x 2j tile.
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane) {
+  uint32_t m = 0x0000ffffu;
+#pragma unroll
+  for (uint32_t j = 16; j != 0; j >>= 1, m ^= m << j) {
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+    x = (lane & j) ? ((x & ~m) | ((y & ~m) >> j)) : ((x & m) | ((y & m) << j));
+  }
+  return x;
+}
+
 // The rest of a round's measurements, after gs_track: the new minimum's
 // state, and on the sampling schedule e / q / suscept (weights `sus`,
-// [nchi][n] in colour order) and packed state samples.
+// [nchi][n] in colour order) and packed state samples.  `xs` (n words of
+// shared memory, or null) holds one chain pair's disagreement word per site
+// while its overlaps are summed.
+// Shared-memory access pattern: the site words are W[s * nw + o], so lanes on
+// consecutive sites read with a stride of nw words (nw-way bank conflicts), and
+// the packed outputs gather through the site permutation.  Bits are therefore
+// packed per 32 consecutive original sites (one gather per replica word, then
+// a ballot or a bit transpose), and the overlap sums first copy each pair's
+// disagreement word to the dense array xs.  Sums keep the order of a warp over sites s = lane +
+// 32 k followed by a shuffle tree, so results do not depend on the CTA size.
 __device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const double* sus, const uint32_t* iperm,
-                             uint32_t i, uint32_t& m_cur, uint32_t& s_cur, GsSnap g) {
+                             uint32_t i, uint32_t& m_cur, uint32_t& s_cur, GsSnap g, uint32_t* xs) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
   const uint32_t n = J.n, nt = J.nt, C = J.C;
   if (g.fresh) {
+    // 64-bit words of the new minimum's spins in original site order, as
+    // 32-bit halves: bit x of half h is site 32 h + x
     const uint32_t nw64 = (n + 63) / 64;
     const uint32_t o = g.c * J.wpc + (g.t >> 5), b = g.t & 31u;
-    for (uint32_t wd = tid; wd < nw64; wd += blockDim.x) {
-      uint64_t v = 0;
-      for (uint32_t x = 0; x < 64 && wd * 64 + x < n; ++x)
-        v |= (uint64_t)((S.W[iperm[wd * 64 + x] * J.nw + o] >> b) & 1u) << x;
-      J.log.words[(size_t)g.k * nw64 + wd] = v;
+    uint32_t* dst = reinterpret_cast<uint32_t*>(J.log.words + (size_t)g.k * nw64);
+    for (uint32_t h = warp; h < 2 * nw64; h += nwarp) {
+      const uint32_t s = h * 32 + lane;
+      const uint32_t bit = s < n ? (S.W[iperm[s] * J.nw + o] >> b) & 1u : 0u;
+      const uint32_t bits = __ballot_sync(0xffffffffu, bit);
+      if (lane == 0) dst[h] = bits;
     }
   }
   const uint32_t P = C / 2;
@@ -1096,39 +1121,79 @@ __device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const d
       const uint32_t c = x / nt, t = x % nt;
       J.out.e[(size_t)t * J.out.M * C + (size_t)m * C + c] = (float)S.Ec[c * J.ntp + t];
     }
-    for (uint32_t y = warp; y < P * nt; y += nwarp) {
-      const uint32_t p = y / nt, t = y % nt;
-      const uint32_t o0 = 2 * p * J.wpc + (t >> 5), o1 = (2 * p + 1) * J.wpc + (t >> 5), b = t & 31u;
-      uint32_t neg = 0;
-      for (uint32_t s = lane; s < n; s += 32) neg += (S.W[s * J.nw + o0] ^ S.W[s * J.nw + o1]) >> b & 1u;
-      for (int off = 16; off > 0; off >>= 1) neg += __shfl_xor_sync(0xffffffffu, neg, off);
-      if (lane == 0) J.out.q[(size_t)t * J.out.M * P + (size_t)m * P + p] = (int32_t)n - 2 * (int32_t)neg;
-      for (uint32_t kx = 0; kx < J.out.nchi; ++kx) {
-        const double* wv = sus + (size_t)kx * n;
-        double chi = 0.0;
-        for (uint32_t s = lane; s < n; s += 32) {
-          const uint32_t x = (S.W[s * J.nw + o0] ^ S.W[s * J.nw + o1]) >> b & 1u;
-          chi += x ? -wv[s] : wv[s];
+    const uint32_t nchi = J.out.nchi;
+    for (uint32_t p = 0; p < P; ++p) {
+      for (uint32_t wd = 0; wd < J.wpc; ++wd) {
+        const uint32_t o0 = 2 * p * J.wpc + wd, o1 = (2 * p + 1) * J.wpc + wd;
+        const uint32_t tn = min(32u, nt - 32 * wd);  // temperatures in this word
+        if (xs) {
+          __syncthreads();  // xs free (previous word's sums done)
+          for (uint32_t s = tid; s < n; s += blockDim.x) xs[s] = S.W[s * J.nw + o0] ^ S.W[s * J.nw + o1];
+          __syncthreads();
         }
-        for (int off = 16; off > 0; off >>= 1) chi += __shfl_xor_sync(0xffffffffu, chi, off);
-        if (lane == 0)
-          J.out.sus[((size_t)t * J.out.nchi + kx) * J.out.M * P + (size_t)m * P + p] = (float)chi;
+        auto xword = [&](uint32_t s) -> uint32_t {
+          return xs ? xs[s] : (S.W[s * J.nw + o0] ^ S.W[s * J.nw + o1]);
+        };
+        // one warp per temperature of the word: q, then the weights in pairs
+        for (uint32_t tb = warp; tb < tn; tb += nwarp) {
+          const uint32_t t = 32 * wd + tb;
+          uint32_t neg = 0;
+          for (uint32_t s = lane; s < n; s += 32) neg += (xword(s) >> tb) & 1u;
+          for (int off = 16; off > 0; off >>= 1) neg += __shfl_xor_sync(0xffffffffu, neg, off);
+          if (lane == 0) J.out.q[(size_t)t * J.out.M * P + (size_t)m * P + p] = (int32_t)n - 2 * (int32_t)neg;
+          for (uint32_t k0 = 0; k0 < nchi; k0 += 2) {
+            double chi[2] = {0.0, 0.0};
+            for (uint32_t s = lane; s < n; s += 32) {
+              const bool flip = (xword(s) >> tb) & 1u;
+#pragma unroll
+              for (uint32_t j = 0; j < 2; ++j)
+                if (k0 + j < nchi) {
+                  const double wv = sus[(size_t)(k0 + j) * n + s];
+                  chi[j] += flip ? -wv : wv;
+                }
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < 2; ++j) {
+              if (k0 + j >= nchi) break;
+              double v = chi[j];
+              for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+              if (lane == 0)
+                J.out.sus[((size_t)t * nchi + k0 + j) * J.out.M * P + (size_t)m * P + p] = (float)v;
+            }
+          }
+        }
       }
     }
   }
   if (sched(J.sample_states, i, J.meas_init, J.num_sweeps)) {
+    // bytes of 8 original sites (bit k = site 8 byte + k).  A warp takes 32
+    // consecutive original sites, gathers each site's replica word once per
+    // chain and word (32 temperatures), and transposes the 32x32 bit block, so
+    // that lane t holds the 32 sites' bits of temperature t: 4 output bytes
     const uint32_t smp = s_cur++;
     const uint32_t nb = (n + 7) / 8;
     const uint32_t Z = J.level == 0 ? nt : (J.level == 1 ? nt / 2 : 1);
-    const uint32_t total = Z * C * nb;
-    for (uint32_t x = tid; x < total; x += blockDim.x) {
-      const uint32_t byte = x % nb, c = (x / nb) % C, z = x / (nb * C);
-      const uint32_t t = J.level == 0 ? z : (J.level == 1 ? nt - 1 - z : nt - 1);
-      const uint32_t o = c * J.wpc + (t >> 5), b = t & 31u;
-      uint32_t v = 0;
-      for (uint32_t bit = 0; bit < 8 && byte * 8 + bit < n; ++bit)
-        v |= ((S.W[iperm[byte * 8 + bit] * J.nw + o] >> b) & 1u) << bit;
-      J.out.samp[(((size_t)z * J.out.S + smp) * C + c) * nb + byte] = (uint8_t)v;
+    for (uint32_t h = warp; h < (n + 31) / 32; h += nwarp) {
+      const uint32_t s = h * 32 + lane;
+      const bool in = s < n;
+      const uint32_t wb = in ? iperm[s] * J.nw : 0u;
+      for (uint32_t c = 0; c < C; ++c) {
+        for (uint32_t wd = 0; wd < J.wpc; ++wd) {
+          const uint32_t x = transpose32(in ? S.W[wb + c * J.wpc + wd] : 0u, lane);
+          const uint32_t t = 32 * wd + lane;
+          uint32_t z = 0xffffffffu;  // sample slot of temperature t, if sampled
+          if (t < nt) {
+            if (J.level == 0) z = t;
+            else if (J.level == 1) z = nt - 1 - t < Z ? nt - 1 - t : 0xffffffffu;
+            else z = t == nt - 1 ? 0u : 0xffffffffu;
+          }
+          if (z != 0xffffffffu) {
+            uint8_t* dst = J.out.samp + (((size_t)z * J.out.S + smp) * C + c) * nb + 4 * h;
+            const uint32_t nk = min(4u, nb - 4 * h);
+            for (uint32_t k = 0; k < nk; ++k) dst[k] = (uint8_t)(x >> (8 * k));
+          }
+        }
+      }
     }
   }
   __syncthreads();
@@ -1137,7 +1202,7 @@ __device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const d
 __device__ void measure_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i, uint32_t& m_cur,
                               uint32_t& s_cur) {
   const GsSnap g = gs_track(J, S, i);
-  measure_rest(J, F, S, F.sus, F.iperm, i, m_cur, s_cur, g);
+  measure_rest(J, F, S, F.sus, F.iperm, i, m_cur, s_cur, g, S.X.D);  // the ICM arrays are free here
 }
 
 // Copy of the job descriptor in shared memory: the phase functions read its
@@ -1296,6 +1361,7 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
       const bool snap = sched(J.sample_states, ip, J.meas_init, J.num_sweeps);
       const double* sus = F.sus;
       const uint32_t* iperm = F.iperm;
+      uint32_t* xs = nullptr;
       if (stage && (g.fresh || meas || snap)) {
         // the measurements gather bits of every site: read the replica words,
         // the weights and the site permutation once into shared memory
@@ -1318,10 +1384,12 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
           for (uint32_t x = tid; x < F.nchi * J.n; x += blockDim.x) ss[x] = F.sus[x];
           sus = ss;
         }
+        st += al16((size_t)F.nchi * J.n * 8);
+        xs = reinterpret_cast<uint32_t*>(st);  // one pair's disagreement words for the overlaps
         __syncthreads();
         S.W = Ws;
       }
-      measure_rest(J, F, S, sus, iperm, ip, m_cur, s_cur, g);
+      measure_rest(J, F, S, sus, iperm, ip, m_cur, s_cur, g, xs);
     }
   }
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
@@ -1592,7 +1660,9 @@ int fused_blocks_per_sm(uint32_t T, size_t smem) {
 
 size_t plain_head_bytes(const PtJob& j, bool stage) {
   size_t b = plain_head_smem(j.n, j.C, j.ntp);
-  if (stage) b += al16((size_t)j.n * j.nw * 4) + al16((size_t)j.n * 4) + al16((size_t)j.F.nchi * j.n * 8);
+  if (stage)
+    b += al16((size_t)j.n * j.nw * 4) + al16((size_t)j.n * 4) + al16((size_t)j.F.nchi * j.n * 8) +
+         al16((size_t)j.n * 4);
   return b;
 }
 
