@@ -306,3 +306,47 @@ def test_pt_fused_and_plain_forms_identical(tb, po, gpu, monkeypatch, kind):
         assert np.array_equal(a, c)
     for a, c in zip(out[0][7], out[1][7]):
         assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize("form", ["fused", "plain"])
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_pt_fast_measurements_match_final_state(tb, po, gpu, monkeypatch, form, level):
+    """The last round is always measured: its packed samples, q and suscept equal
+    what the final state gives, and the last ground-state snapshot has the
+    recorded energy.  49 sites (a partial output byte and 32-site block), 40
+    temperatures (a partial replica word) and 4 chains (two overlap pairs)."""
+    L, nt, C, sweeps = 7, 40, 4, 60
+    text = gi.lattice(L, 2, "gauss", 21)
+    w = np.stack([gi.fourier_weights(L, 2, 0), gi.fourier_weights(L, 2, 1), 0.25 * gi.fourier_weights(L, 2, 0)])
+    h = tb.HostInstance.parse(text)
+    for row in w:
+        h.add_suscept(row)
+    b = po.geometric_betas(0.2, 5.0, nt)
+    monkeypatch.setenv("TAMC_PT_FORM", form)
+    run = tb.PtRun(gpu.upload(h), _pt(tb, sweeps, b, nt // 2, C, 8, 7, 9, level), 31).run().sync()
+    spins, _ = run.state()                      # [C][nt][n], +-1
+    n = spins.shape[-1]
+    ts = run.samples()
+    smp = np.array(ts.samples)                  # [Z][S*C][ceil(n/8)]
+    Z = {0: nt, 1: nt // 2, 2: 1}[level]
+    assert smp.shape[0] == Z
+    S = smp.shape[1] // C
+    for z in range(Z):
+        t = {0: z, 1: nt - 1 - z, 2: nt - 1}[level]
+        for c in range(C):
+            bits = np.unpackbits(smp[z, (S - 1) * C + c], bitorder="little")[:n]
+            assert np.array_equal(1 - 2 * bits.astype(np.int8), spins[c, t]), (z, c)
+    P = C // 2
+    q = np.array(ts.q)                          # [nt][M*P]
+    sus = np.array(ts.suscept)                  # [nt][nchi][M*P]
+    M = q.shape[1] // P
+    for p in range(P):
+        ov = spins[2 * p].astype(np.int64) * spins[2 * p + 1]   # [nt][n]
+        assert np.array_equal(q[:, (M - 1) * P + p], ov.sum(axis=1))
+        chi = ov.astype(np.float64) @ w.T                        # [nt][nchi]
+        got = sus[:, :, (M - 1) * P + p].astype(np.float64)
+        assert np.all(np.abs(got - chi) <= 1e-5 * np.maximum(np.abs(chi), 1.0))
+    steps, en, words = run.gs()
+    last = np.unpackbits(words[-1].view(np.uint8), bitorder="little")[:n]
+    s = (1 - 2 * last.astype(np.int8))[None]
+    assert _rel_ok(np.array([en[-1]]), _f64_energies(po, text, s).reshape(1))
