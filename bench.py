@@ -16,6 +16,9 @@ seeded synthetic data), a linear beta schedule 0.1 -> 10 over 1000 sweeps and
   roofline: HBM bound of the per-flip algorithmic bytes (one spin bit read and
           written, plus the CSR row of the site amortised over the restarts
           sharing one pass): B = 2/8 + (4 + 8*3 + 4)/1024 bytes per flip.
+  issue_roofline: the bound that binds (state stays in shared memory): warp
+          instructions per launch from the committed ncu summary over the live
+          launch time, against 4 issue slots per SM per cycle at the sampled clock.
   cpu_baseline: the CPU restatement of the reference (oracle/, OpenMP over
           SA partitions as the reference's rayon code), on a bounded sample
           of the same schedule.
@@ -61,15 +64,20 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _profile_traffic():
-    """dram bytes per launch of the SA kernel from the committed ncu summary, if present."""
+def _profile_value(key):
+    """A per-launch figure of the SA kernel (`key: value` line) from the committed ncu summary, if present."""
     path = os.path.join(ROOT, "profiles", "sa_fast_c2.md")
     try:
         txt = open(path).read()
-        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+        m = re.search(key + r":\s*([0-9.eE+]+)", txt)
         return float(m.group(1)) if m else None
     except OSError:
         return None
+
+
+def _profile_traffic():
+    """dram bytes per launch of the SA kernel from the committed ncu summary, if present."""
+    return _profile_value("traffic_bytes_per_launch")
 
 
 class ClockSampler:
@@ -261,6 +269,19 @@ def run_gpu(args):
         per_launch_ms = float(np.mean(times))
         achieved = BYTES_PER_FLIP * FLIPS_PER_STEP / (per_launch_ms / 1e3) / 1e9
         traffic = _profile_traffic()
+        clocks = clk.summary()
+        # The kernel keeps its state on chip, so instruction issue binds, not HBM:
+        # warp instructions per launch (ncu, same workload and tile) over the live
+        # launch time, against 4 issue slots per SM per cycle at the sampled clock.
+        inst = _profile_value("warp_instructions_per_launch")
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+        issue = None
+        if inst and mhz:
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            ach, pk = inst / (per_launch_ms / 1e3), sms * 4 * mhz * 1e6
+            issue = {"achieved": ach, "peak": pk, "unit": "warp instructions/s", "frac": ach / pk,
+                     "instructions_per_launch": inst, "clock_mhz": mhz,
+                     "source": "profiles/sa_fast_c2.md (smsp__inst_executed.sum of one launch)"}
         out = {"metric": METRIC, "value": value, "unit": "flips/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
@@ -270,7 +291,8 @@ def run_gpu(args):
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{kind} burst",
                             "bytes_per_flip": BYTES_PER_FLIP},
-               "clocks": clk.summary(), "best_energy": e_min, "restarts_at_best": frac_best,
+               "issue_roofline": issue,
+               "clocks": clocks, "best_energy": e_min, "restarts_at_best": frac_best,
                "tts99_s": per_launch_ms / 1e3 * (1.0 if p_anneal >= 0.99 else
                                                 math.log(0.01) / math.log(1.0 - p_anneal))}
         if not args.no_cpu and world == 1:
