@@ -1166,32 +1166,41 @@ __device__ void measure_rest(const PtJob& J, const FastInst& F, Smem& S, const d
     }
   }
   if (sched(J.sample_states, i, J.meas_init, J.num_sweeps)) {
-    // bytes of 8 original sites (bit k = site 8 byte + k).  A warp takes 32
-    // consecutive original sites, gathers each site's replica word once per
-    // chain and word (32 temperatures), and transposes the 32x32 bit block, so
-    // that lane t holds the 32 sites' bits of temperature t: 4 output bytes
+    // bytes of 8 original sites (bit k = site 8 byte + k).  A warp takes 8
+    // blocks of 32 consecutive original sites for one chain and replica word,
+    // gathers each site's word once and transposes each 32x32 bit block, so
+    // that lane t holds 32 bytes of temperature t's row: two 16-byte stores
+    // per row where the rows are 16-byte aligned, else byte stores.
     const uint32_t smp = s_cur++;
     const uint32_t nb = (n + 7) / 8;
     const uint32_t Z = J.level == 0 ? nt : (J.level == 1 ? nt / 2 : 1);
-    for (uint32_t h = warp; h < (n + 31) / 32; h += nwarp) {
-      const uint32_t s = h * 32 + lane;
-      const bool in = s < n;
-      const uint32_t wb = in ? iperm[s] * J.nw : 0u;
-      for (uint32_t c = 0; c < C; ++c) {
-        for (uint32_t wd = 0; wd < J.wpc; ++wd) {
-          const uint32_t x = transpose32(in ? S.W[wb + c * J.wpc + wd] : 0u, lane);
-          const uint32_t t = 32 * wd + lane;
-          uint32_t z = 0xffffffffu;  // sample slot of temperature t, if sampled
-          if (t < nt) {
-            if (J.level == 0) z = t;
-            else if (J.level == 1) z = nt - 1 - t < Z ? nt - 1 - t : 0xffffffffu;
-            else z = t == nt - 1 ? 0u : 0xffffffffu;
-          }
-          if (z != 0xffffffffu) {
-            uint8_t* dst = J.out.samp + (((size_t)z * J.out.S + smp) * C + c) * nb + 4 * h;
-            const uint32_t nk = min(4u, nb - 4 * h);
-            for (uint32_t k = 0; k < nk; ++k) dst[k] = (uint8_t)(x >> (8 * k));
-          }
+    const uint32_t nblk = ((n + 31) / 32 + 7) / 8;
+    const bool wide = nb % 16 == 0;  // row starts 16-byte aligned (the buffer itself is)
+    for (uint32_t it = warp; it < C * J.wpc * nblk; it += nwarp) {
+      const uint32_t hb = it % nblk, cw = it / nblk, c = cw / J.wpc, wd = cw % J.wpc;
+      uint32_t xv[8];
+#pragma unroll
+      for (uint32_t j = 0; j < 8; ++j) {
+        const uint32_t s = (8 * hb + j) * 32 + lane;
+        xv[j] = transpose32(s < n ? S.W[iperm[s] * J.nw + c * J.wpc + wd] : 0u, lane);
+      }
+      const uint32_t t = 32 * wd + lane;
+      uint32_t z = 0xffffffffu;  // sample slot of temperature t, if sampled
+      if (t < nt) {
+        if (J.level == 0) z = t;
+        else if (J.level == 1) z = nt - 1 - t < Z ? nt - 1 - t : 0xffffffffu;
+        else z = t == nt - 1 ? 0u : 0xffffffffu;
+      }
+      if (z != 0xffffffffu) {
+        uint8_t* dst = J.out.samp + (((size_t)z * J.out.S + smp) * C + c) * nb + 32 * hb;
+        if (wide && 32 * hb + 32 <= nb) {
+          reinterpret_cast<uint4*>(dst)[0] = make_uint4(xv[0], xv[1], xv[2], xv[3]);
+          reinterpret_cast<uint4*>(dst)[1] = make_uint4(xv[4], xv[5], xv[6], xv[7]);
+        } else {
+#pragma unroll
+          for (uint32_t j = 0; j < 8; ++j)
+            for (uint32_t k = 0; k < 4; ++k)
+              if (32 * hb + 4 * j + k < nb) dst[4 * j + k] = (uint8_t)(xv[j] >> (8 * k));
         }
       }
     }
