@@ -392,17 +392,40 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
       if (tid == 0) X.cnt[b] = cnt;
     }
   } else {
-    // several slots: one warp per slot, ballot scans in site order
+    // several slots: one warp per slot, ballot scans in site order.  Up to 32
+    // chunks of 32 sites, lane L keeps chunk L's count, and a prefix sum over the
+    // lanes finds the chunk of the k-th site (no second scan)
+    const uint32_t nchunk = (n + 31) / 32;
     for (uint32_t b = warp; b < 32; b += nwarp) {
       if (!((gmask >> b) & 1u)) continue;
-      uint32_t cnt = 0;
-      for (uint32_t base = 0; base < n; base += 32) {
-        const uint32_t s = base + lane;
-        cnt += __popc(__ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u)));
+      const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;  // needed only if cnt > 0
+      uint32_t cnt = 0, cc = 0;
+#pragma unroll 4
+      for (uint32_t ch = 0; ch < nchunk; ++ch) {
+        const uint32_t s = ch * 32 + lane;
+        const uint32_t c = __popc(__ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u)));
+        cnt += c;
+        if (ch == lane) cc = c;
       }
       if (cnt == 0) continue;
-      const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;
       uint32_t k = (uint32_t)(((uint64_t)u * cnt) >> 32);
+      if (nchunk <= 32) {
+        uint32_t incl = cc;
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= (uint32_t)o) incl += v;
+        }
+        const uint32_t excl = incl - cc;
+        const uint32_t ch = __ffs(__ballot_sync(0xffffffffu, k >= excl && k < incl)) - 1;  // exactly one chunk
+        const uint32_t kk = k - __shfl_sync(0xffffffffu, excl, ch);
+        const uint32_t s = ch * 32 + lane;
+        const uint32_t bal = __ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u));
+        if (lane == 0) {
+          X.seed[b] = ch * 32 + __fns(bal, 0, (int)kk + 1);
+          X.cnt[b] = cnt;
+        }
+        continue;
+      }
       for (uint32_t base = 0; base < n; base += 32) {
         const uint32_t s = base + lane;
         const uint32_t bal = __ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u));
