@@ -541,10 +541,9 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     if (tid < 32 && ((gmask >> tid) & 1u) && X.cnt[tid]) atomicOr(&XC[X.seed[tid]], 1u << tid);
     __syncthreads();
     // Square and cubic lattices: per-thread state in registers (the fused
-    // kernel has registers for 2 sites of 4 entries per thread, and spills a
-    // few bytes elsewhere for it: measured 1.3x faster on 2-D L=32 all the
-    // same); otherwise rows of 4 or 6 entries still load all their columns,
-    // then all the neighbours' words, before use.
+    // kernel has registers for 2 sites of 4 entries per thread); otherwise
+    // rows of 4 or 6 entries still load all their columns, then all the
+    // neighbours' words, before use.
     const uint32_t udeg = F.udeg;
     if (PLAIN && udeg == 4) {
       prop_passes<4, 4, true>(n, T, tid, XD, XC, col);
