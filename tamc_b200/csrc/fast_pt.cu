@@ -222,18 +222,6 @@ __device__ void full_energies(const PtJob& J, const FastInst& F, Smem& S, uint32
 // rounds end within n + 1, and the final labels are the smallest site index
 // of each component whatever the thread schedule was.
 
-__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  uint32_t t = 0;
-  for (uint32_t k = 0; k < nw; ++k) t += red[k];
-  __syncthreads();
-  return t;
-}
-
 // Houdayer move (src/pt.rs:31-77) for the slots of `gmask` (bits of word w)
 // of chain pair (c0, c1) at sweep i: count the q<0 sites of every slot, draw
 // the seed index from Philox, find the seed's component of the q<0 subgraph,
@@ -362,32 +350,42 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
   __syncthreads();
   const uint32_t G = __popc(gmask);
   if (G == 1) {
-    // one slot: block-wide count and ordered search for the k-th q<0 site
+    // one slot: each warp counts a contiguous segment of sites with ballots,
+    // one warp-wide prefix sum over the segment counts orders them, and the
+    // warp whose segment holds the k-th q<0 site finds it
     const uint32_t b = __ffs(gmask) - 1;
-    const uint32_t chunk = (n + T - 1) / T, s0 = min(n, tid * chunk), s1 = min(n, s0 + chunk);
-    uint32_t mine = 0;
-    for (uint32_t s = s0; s < s1; ++s) mine += (XD[s] >> b) & 1u;
-    const uint32_t cnt = block_sum(mine, X.red);
+    const uint32_t seg = ((n + nwarp - 1) / nwarp + 31u) & ~31u;
+    const uint32_t w0 = min(n, warp * seg), w1 = min(n, w0 + seg);
+    uint32_t wc = 0;
+    for (uint32_t base = w0; base < w1; base += 32) {
+      const uint32_t s = base + lane;
+      wc += __popc(__ballot_sync(0xffffffffu, s < w1 && ((XD[s] >> b) & 1u)));
+    }
+    if (lane == 0) X.red[warp] = wc;
+    __syncthreads();
+    const uint32_t v = lane < nwarp ? X.red[lane] : 0u;
+    uint32_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    const uint32_t cnt = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t before = __shfl_sync(0xffffffffu, incl - v, warp);
     if (cnt) {
       const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;
       const uint32_t k = (uint32_t)(((uint64_t)u * cnt) >> 32);
-      // exclusive prefix of the per-thread counts
-      uint32_t incl = mine;
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (uint32_t)o) incl += v;
-      }
-      if (lane == 31) X.red[warp] = incl;
-      __syncthreads();
-      uint32_t before = incl - mine;
-      for (uint32_t k2 = 0; k2 < warp; ++k2) before += X.red[k2];
-      if (k >= before && k < before + mine) {
+      if (k >= before && k < before + wc) {
         uint32_t r = k - before;
-        for (uint32_t s = s0; s < s1; ++s)
-          if ((XD[s] >> b) & 1u) {
-            if (r == 0) { X.seed[b] = s; break; }
-            --r;
+        for (uint32_t base = w0; base < w1; base += 32) {
+          const uint32_t s = base + lane;
+          const uint32_t bal = __ballot_sync(0xffffffffu, s < w1 && ((XD[s] >> b) & 1u));
+          const uint32_t c = __popc(bal);
+          if (r < c) {
+            if (lane == 0) X.seed[b] = base + __fns(bal, 0, (int)r + 1);
+            break;
           }
+          r -= c;
+        }
       }
       if (tid == 0) X.cnt[b] = cnt;
     }
