@@ -49,19 +49,23 @@ int tamc_gpu_sa_run_noalloc(tamc_inst* inst, const float* d_betas, uint32_t nbet
   const uint32_t R = num_replicas;
   if (!R) return TAMC_OK;
   if (!d_energies || !d_packed) fail(TAMC_E_INVAL, "null argument");
-  const uint64_t need = (uint64_t)((R + 31) / 32) * inst->n * 4;
+  // 64-bit throughout: R + 31 must not wrap for R near 2^32
+  const uint64_t need = (((uint64_t)R + 31) / 32) * (uint64_t)inst->n * 4;
   if (need > TAMC_SA_NOALLOC_SCRATCH_BYTES)
     fail(TAMC_E_INVAL, "num_replicas " + std::to_string(R) + " x n " + std::to_string(inst->n) + " needs " +
                            std::to_string(need) + " bytes of replica words, above the static scratch of " +
                            std::to_string((uint64_t)TAMC_SA_NOALLOC_SCRATCH_BYTES) + " bytes");
   tamc_gpu* g = inst->g;
+  SaFastArgs a;
+  a.F = make_fast_inst(inst);
+  // the shared-memory check sa_fast_choose makes, before anything is queued
+  const SaTile tile = sa_fast_peek(g, a.F, R);
+  if (tile.smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the fast SA kernel");
   TAMC_CUDA(cudaSetDevice(g->device));
   uint32_t* words = words_on(g->device);
   cudaStream_t st = stream ? (cudaStream_t)stream : g->stream;
   // the anneal kernel ORs the final spins into the words: they start at zero
   TAMC_CUDA(cudaMemsetAsync(words, 0, need, st));
-  SaFastArgs a;
-  a.F = make_fast_inst(inst);
   a.betas = d_betas;
   a.nbeta = nbeta;
   a.key = philox_key(seed);
@@ -69,7 +73,7 @@ int tamc_gpu_sa_run_noalloc(tamc_inst* inst, const float* d_betas, uint32_t nbet
   a.init_words = nullptr;
   a.words_out = words;
   a.energies_out = d_energies;
-  sa_fast_launch(st, a, sa_fast_peek(g, a.F, R));
+  sa_fast_launch(st, a, tile);
   sa_pack_states(st, words, inst->n, R, d_packed);
   g->count(2);
   TAMC_API_END

@@ -33,11 +33,26 @@ def test_noalloc_matches_sa_run_on_consecutive_calls(tb, gpu):
         d = gpu.upload(tb.HostInstance.parse(text))
         runs.append((d, R, seed) + _device_buffers(torch, R, d.n))
     torch.cuda.synchronize()
-    # two calls back to back on one stream, both on shapes the existing entry
-    # point has not tuned yet (heuristic tile); the second reuses the scratch
-    for d, R, seed, de, dp in runs:
-        tb.sa_run_noalloc(d, db.data_ptr(), len(betas), R, seed, de.data_ptr(), dp.data_ptr(), stream.cuda_stream)
-    stream.synchronize()
+
+    def call_all():
+        # two calls back to back on one stream; the second reuses the scratch
+        for d, R, seed, de, dp in runs:
+            tb.sa_run_noalloc(d, db.data_ptr(), len(betas), R, seed, de.data_ptr(), dp.data_ptr(),
+                              stream.cuda_stream)
+        stream.synchronize()
+
+    # first round: both shapes are new to the existing entry point (heuristic
+    # tile); loading the kernels on first launch may take device memory
+    call_all()
+    free0 = torch.cuda.mem_get_info()[0]
+    for d, R, seed, de, dp in runs:  # garbage again, so the repeat must rewrite every output
+        de.fill_(float("nan"))
+        dp.fill_(0xA5)
+    torch.cuda.synchronize()
+    call_all()
+    call_all()
+    # the defining property: calls after the first take no device memory
+    assert torch.cuda.mem_get_info()[0] == free0
     for d, R, seed, de, dp in runs:
         e_ref, packed_ref = tb.sa_run(d, betas, R, 1, seed)
         assert np.array_equal(de.cpu().numpy().view(np.uint32), e_ref.view(np.uint32))
@@ -53,6 +68,32 @@ def test_noalloc_rejects_shapes_beyond_static_scratch(tb, gpu):
     R = 32 * 1024
     betas = torch.ones(4, dtype=torch.float32, device="cuda")
     de, dp = _device_buffers(torch, 1, 2000)
+    for R in (32 * 1024, 0xFFFFFFFF):  # the largest count must not wrap to a small need
+        with pytest.raises(tb.TamcError) as err:
+            tb.sa_run_noalloc(d, betas.data_ptr(), 4, R, 1, de.data_ptr(), dp.data_ptr())
+        assert err.value.code == -1 and "static scratch" in str(err.value)
+
+
+def test_noalloc_rejects_instances_beyond_shared_memory(tb, gpu):
+    """A ring of 200000 sites fits the static scratch at 32 replicas (800 KB of
+    words) but not the annealing kernel's shared memory: the call must fail
+    with UNSUPPORTED, as tamc_gpu_sa_run does, before it queues any work."""
+    torch = pytest.importorskip("torch")
+    n = 200_000
+    i = np.arange(n)
+    nb = np.sort(np.stack([(i - 1) % n, (i + 1) % n], 1), axis=1)
+    rp = np.arange(0, 2 * n + 1, 2, dtype=np.uint32)
+    h = tb.HostInstance.from_csr(rp, nb.ravel().astype(np.uint32), np.ones(2 * n, np.float32),
+                                 np.zeros(n, np.float32))
+    d = gpu.upload(h)
+    betas = torch.ones(4, dtype=torch.float32, device="cuda")
+    de, dp = _device_buffers(torch, 32, n)
+    torch.cuda.synchronize()
     with pytest.raises(tb.TamcError) as err:
-        tb.sa_run_noalloc(d, betas.data_ptr(), 4, R, 1, de.data_ptr(), dp.data_ptr())
-    assert err.value.code == -1 and "static scratch" in str(err.value)
+        tb.sa_run_noalloc(d, betas.data_ptr(), 4, 32, 1, de.data_ptr(), dp.data_ptr())
+    assert err.value.code == -7 and "too large" in str(err.value)
+    torch.cuda.synchronize()
+    assert torch.isnan(de).all()  # nothing ran
+    with pytest.raises(tb.TamcError) as err:
+        tb.sa_run(d, np.ones(4, np.float32), 32, 1, 1)
+    assert err.value.code == -7
