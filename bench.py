@@ -1,36 +1,50 @@
-"""Benchmark: spin-flip attempts per second of simulated annealing on one B200.
+"""Benchmark: spin-flip attempts per second of batched PT-ICM against the plain
+form, on one B200.
 
-Workload (the configuration the headline metric is quoted on): simulated
-annealing of a sparse random Ising problem -- N=2000 spins on a random
-3-regular graph, couplings J_ij ~ N(0,1) and biases h_i ~ N(0, 0.1^2) (f32,
-seeded synthetic data), a linear beta schedule 0.1 -> 10 over 1000 sweeps and
-1024 independent restarts.  One step = one full anneal of all restarts =
-2000 * 1024 * 1000 = 2.048e9 flip attempts.
+Default workload (--workload batch_c3): 256 uneven 2-D +-J spin-glass
+instances -- periodic L x L lattices with L drawn uniformly from
+{8, 12, 16, 24, 32}, J_ij uniform in {-1, +1} (f32, seeded synthetic data) --
+each a PT-ICM run with a geometric beta ladder 0.2 -> 5.0 of 16, 24 or 32
+temperatures (drawn uniformly), 2 replica chains, Houdayer moves from
+lo_beta = 1.0, 5000 sweeps.  One step = the whole batch run to the end =
+sum_j L_j^2 * nt_j * 2 * 5000 flip attempts (about 2.5e10).
 
-  value : device-resident throughput: instance, schedule and outputs already in
-          HBM, kernel time from CUDA events on the launching stream; L2 is
-          flushed (a 256 MiB write) between timed steps.
-  e2e   : the same anneal through the reference-facing C ABI call with host
-          buffers (tamc_gpu_sa_run: host schedule in, host energies and
-          bit-packed states out), copies inside the timed region.
-  roofline: HBM bound of the per-flip algorithmic bytes (one spin bit read and
-          written, plus the CSR row of the site amortised over the restarts
-          sharing one pass): B = 2/8 + (4 + 8*3 + 4)/1024 bytes per flip.
-  issue_roofline: the bound that binds (state stays in shared memory): warp
-          instructions per launch from the committed ncu summary over the live
-          launch time, against 4 issue slots per SM per cycle at the sampled clock.
-  cpu_baseline: the CPU restatement of the reference (oracle/, OpenMP over
-          SA partitions as the reference's rayon code), on a bounded sample
-          of the same schedule.
+  value   : batched form (tamc_gpu_batch_*: all jobs in one persistent kernel
+            per chunk of rounds, each chunk a replayed CUDA graph), instances
+            resident in HBM; CUDA events on the library's stream around the
+            whole run, L2 flushed (256 MiB write) between steps.
+  plain_flips_per_s / batched_over_plain : the plain form (one instance at a
+            time, one launch per sweep phase) on a fixed systematic sample of
+            the same jobs, same seeds, CUDA-event time.
+  e2e     : the same batch through the C ABI from host instances: upload every
+            instance, create the batch, run, read every job's ground-state
+            trajectory and acceptance counts, free; wall clock, with the
+            library's own count of host<->device bytes.
+  roofline: HBM bound of the per-flip algorithmic bytes, job by job
+            B_j = 2/8 + (4 + 8*4 + 4) / (2 nt_j) (one spin bit read and written,
+            plus the CSR row of the site amortised over the replicas sharing
+            one pass), over the device time of the chunk launches.
+  issue_roofline: the bound that applies (the replicas stay in shared memory):
+            warp instructions per step from the committed ncu summary over the
+            same device time, against 4 issue slots per SM per cycle.
+  cpu_baseline: the CPU restatement of the reference (oracle/) on a fixed
+            subset of the same jobs at their full 5000 sweeps, one job per host
+            thread on all cores, median of 3 runs, in a child process.
+  c4      : 3-D L=16 Gaussian PT-ICM (64 temperatures, 20000 sweeps, samples
+            every 32) on the GPU, against whole oracle runs of the same method
+            with fewer sweeps on all cores (gpu_over_cpu).
 
-`--impl reference` times that CPU implementation on the same workload and
-prints the reference arm's line.  Under torchrun (N > 1) every rank anneals
-its own 1024 restarts (independent seeds; weak scaling, no collective on the
-data path) and the line reports all ranks' flips over the slowest rank's time.
+`--impl reference` times the CPU restatement on the same jobs and prints the
+reference arm's line.  `--workload sa_c2 | pt_c1 | pt_c4 | serve_c5` measures
+the other configurations (one JSON line each).  Under torchrun (N > 1) every
+rank runs its own 256-job batch (same shapes, its own couplings and seeds; weak
+scaling, no collective on the data path) and the line reports all ranks'
+flips over the slowest rank's time.
 """
 from __future__ import annotations
 
 import argparse
+import concurrent.futures as cf
 import json
 import math
 import os
@@ -45,16 +59,16 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_SPINS, DEGREE, N_REPLICAS, N_SWEEPS = 2000, 3, 1024, 1000
-BETA0, BETA1 = 0.1, 10.0
-FLIPS_PER_STEP = N_SPINS * N_REPLICAS * N_SWEEPS
-BYTES_PER_FLIP = 2 / 8 + (4 + 8 * DEGREE + 4) / N_REPLICAS
-METRIC = "spin-flip attempts/s (SA, 1 B200)"
-CONFIG = {"workload": "SA: N=2000 random 3-regular Ising, J~N(0,1), h~N(0,0.01), linear beta 0.1->10 x 1000 "
-                      "sweeps, 1024 restarts", "n": N_SPINS, "degree": DEGREE, "restarts": N_REPLICAS,
-          "sweeps": N_SWEEPS, "l2": "flushed between timed steps (256 MiB write)"}
+METRIC = "spin-flip attempts/s (batched PT-ICM vs plain, 1 B200)"
+C3_JOBS, C3_SWEEPS = 256, 5000
+C3_L, C3_NT = (8, 12, 16, 24, 32), (16, 24, 32)
+C3_CONFIG = {"workload": "batch_c3: 256 uneven 2-D +-J PT-ICM instances, L~U{8,12,16,24,32} periodic, "
+                         "nt~U{16,24,32} geometric beta 0.2->5.0, 2 chains, ICM from beta 1.0, 5000 sweeps",
+             "instances": C3_JOBS, "sweeps": C3_SWEEPS, "chains": 2, "mode": "colour-ordered (TAMC_MODE_FAST)",
+             "l2": "flushed between timed steps (256 MiB write)"}
 
 
+# ------------------------------------------------------------ helpers ----
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -64,20 +78,14 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _profile_value(key):
-    """A per-launch figure of the SA kernel (`key: value` line) from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "sa_fast_c2.md")
+def _profile_value(name, key):
+    """A `key: value` figure from a committed ncu summary under profiles/, if present."""
     try:
-        txt = open(path).read()
+        txt = open(os.path.join(ROOT, "profiles", name)).read()
         m = re.search(key + r":\s*([0-9.eE+]+)", txt)
         return float(m.group(1)) if m else None
     except OSError:
         return None
-
-
-def _profile_traffic():
-    """dram bytes per launch of the SA kernel from the committed ncu summary, if present."""
-    return _profile_value("traffic_bytes_per_launch")
 
 
 class ClockSampler:
@@ -132,46 +140,176 @@ def _dist():
     return world, rank, local
 
 
-def cpu_sample(text: str, betas: np.ndarray, budget_s: float = 12.0, threads: int | None = None):
-    """Times the oracle (CPU restatement of the reference, all host threads) on a
-    bounded, schedule-spread sample of the workload: all 1024 restarts, a
-    strided subset of the 1000 betas.  Returns (flips/s, description, cores)."""
+def _child_json(argv, timeout=900):
+    """Runs `python bench.py <argv>` in a fresh process (no torch, no CUDA
+    context, its own OpenMP runtime) and returns the JSON it prints last."""
+    r = subprocess.run([sys.executable, os.path.abspath(__file__)] + argv, capture_output=True, text=True,
+                       timeout=timeout, cwd=ROOT)
+    if r.returncode != 0:
+        raise RuntimeError(f"CPU leg failed: {r.stderr[-2000:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+# ------------------------------------------------------- C3 job list ----
+def c3_jobs(rank: int = 0):
+    """(L, nt, instance seed, run seed) of the 256 jobs; shapes are the same on
+    every rank, couplings and run seeds differ per rank."""
+    rng = np.random.default_rng(0)
+    out = []
+    for k in range(C3_JOBS):
+        L = int(rng.choice(C3_L))
+        nt = int(rng.choice(C3_NT))
+        out.append((L, nt, 1000 + k + 100003 * rank, 7 + k + 100003 * rank))
+    return out
+
+
+def c3_flips(jobs, sweeps=C3_SWEEPS):
+    return sum(L * L * nt * 2 * sweeps for L, nt, _, _ in jobs)
+
+
+def c3_bytes(jobs, sweeps=C3_SWEEPS):
+    """Algorithmic HBM bytes of the jobs: per flip 2/8 + (4 + 8*4 + 4)/R, R = 2 nt."""
+    return sum(L * L * nt * 2 * sweeps * (0.25 + 40.0 / (2 * nt)) for L, nt, _, _ in jobs)
+
+
+def _lattice_params(tb, nt, sweeps, sample=None, states=None, level=0, threads=8):
+    b = tb.geometric_betas(0.2, 5.0, nt)
+    lo = int(np.argmax(b >= np.float32(1.0))) if np.any(b >= np.float32(1.0)) else nt - 1
+    return tb.PtParams(sweeps, b, lo, 0.5, True, 2, threads, sample, states, level)
+
+
+# ---------------------------------------------------- CPU (oracle) legs ----
+def cpu_c3(stride: int, runs: int, threads: int | None = None):
+    """The oracle (CPU restatement of the reference) on jobs 0, stride, 2*stride, ...
+    of the batch, each a whole 5000-sweep run; one job per host thread (a
+    thread pool over ctypes calls, which release the GIL), longest jobs first.
+    Returns the per-run flips/s and a description."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
+    from tamc_b200 import instances as gi
     cores = threads or os.cpu_count() or 1
-    inst = po.Instance.from_text(text)
-    probe = betas[:: max(1, len(betas) // 4)][:4]
+    jobs = c3_jobs()[::stride]
+    texts = [gi.lattice(L, 2, "pm", si) for L, _, si, _ in jobs]
+    insts = [po.Instance.from_text(t) for t in texts]
+    order = sorted(range(len(jobs)), key=lambda k: -jobs[k][0] ** 2 * jobs[k][1])
+    flips = c3_flips(jobs)
+
+    def one(k):
+        L, nt, _, seed = jobs[k]
+        b = po.geometric_betas(0.2, 5.0, nt)
+        lo = po.lo_beta_idx(b, lo_beta=1.0)
+        r = po.PtRun(insts[k], b, C3_SWEEPS, 0.5, lo, True, 2, 8, seed=seed)
+        r.run(nthreads=1)
+        return r.gs()[-1][1] if r.gs() else None
+
+    rates = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+            list(ex.map(one, order))
+        rates.append(flips / (time.perf_counter() - t0))
+    desc = (f"oracle PT-ICM (method as the GPU run, threads: 8 semantics), {len(jobs)} of the 256 jobs "
+            f"(every {stride}th), 5000 sweeps each, {flips:.3g} flips per run, one job per thread on {cores} "
+            f"threads, median of {runs} runs in a child process")
+    return rates, desc, cores
+
+
+def cpu_c4(sweeps: int, runs: int, threads: int | None = None):
+    """Whole oracle runs of the C4 method (run_parallel, threads: 64) with `sweeps`
+    sweeps on all host cores (OpenMP over the replicas)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from tamc_b200 import instances as gi
+    cores = threads or os.cpu_count() or 1
+    L = 16
+    inst = po.Instance.from_text(gi.lattice(L, 3, "gauss", 0))
+    for ax in (0, 1):
+        inst.add_suscept(gi.fourier_weights(L, 3, ax))
+    b = po.geometric_betas(0.2, 5.0, 64)
+    lo = po.lo_beta_idx(b, lo_beta=1.0)
+    rates = []
+    for k in range(runs):
+        r = po.PtRun(inst, b, sweeps, 0.5, lo, True, 2, 64, sample=32, sample_states=32, sample_limiting=0,
+                     seed=3 + k)
+        t0 = time.perf_counter()
+        r.run(nthreads=cores)
+        rates.append(4096 * 64 * 2 * sweeps / (time.perf_counter() - t0))
+    desc = (f"oracle run_parallel (threads: 64), whole runs of {sweeps} sweeps (warm-up 0.5, samples every 32), "
+            f"{cores} OpenMP threads, median of {runs} runs in a child process")
+    return rates, desc, cores
+
+
+def cpu_sa(budget_s: float, threads: int | None = None):
+    """The oracle's SA on whole anneals of the C2 instance (all 1000 betas) with as
+    many of the 1024 restarts as fit the budget, in `cores` partitions."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    from tamc_b200 import instances as gi
+    cores = threads or os.cpu_count() or 1
+    inst = po.Instance.from_text(gi.sa_regular(2000, 3, 0))
+    betas = np.linspace(0.1, 10.0, 1000).astype(np.float32)
     t0 = time.perf_counter()
-    po.sa_run(inst, probe, N_REPLICAS, cores, 1, nthreads=cores)
-    per_sweep = (time.perf_counter() - t0) / len(probe)
-    k = int(min(len(betas), max(4, budget_s / max(per_sweep, 1e-9))))
-    sample = betas[np.linspace(0, len(betas) - 1, k).astype(int)]
-    t0 = time.perf_counter()
-    po.sa_run(inst, sample, N_REPLICAS, cores, 2, nthreads=cores)
-    dt = time.perf_counter() - t0
-    flips = N_SPINS * N_REPLICAS * len(sample)
-    desc = (f"oracle SA, {N_REPLICAS} restarts in {cores} partitions x {len(sample)} of the 1000 betas "
-            f"(evenly spread), {flips:.3g} flips in {dt:.1f} s")
-    return flips / dt, desc, cores
+    po.sa_run(inst, betas, cores, cores, 1, nthreads=cores)  # one restart per thread
+    per = time.perf_counter() - t0
+    reps = int(max(1, min(1024 // cores, budget_s / max(per, 1e-9))))
+    R = reps * cores
+    rates = []
+    for k in range(3):
+        t0 = time.perf_counter()
+        po.sa_run(inst, betas, R, cores, 2 + k, nthreads=cores)
+        rates.append(2000 * R * 1000 / (time.perf_counter() - t0))
+    desc = (f"oracle SA run_parallel, whole anneals (all 1000 betas) of {R} of the 1024 restarts in {cores} "
+            f"partitions, median of 3 runs in a child process")
+    return rates, desc, cores
+
+
+def run_cpu_leg(args):
+    if args.cpu_leg == "c3":
+        rates, desc, cores = cpu_c3(args.cpu_stride, args.cpu_runs)
+    elif args.cpu_leg == "c4":
+        rates, desc, cores = cpu_c4(args.c4_cpu_sweeps, args.cpu_runs)
+    else:
+        rates, desc, cores = cpu_sa(args.cpu_budget)
+    print(json.dumps({"value": float(np.median(rates)), "runs": rates, "sample": desc, "cores": cores}))
+    return 0
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference on the C3 jobs,
+    on rank 0 only (other ranks exit without work)."""
     world, rank, _ = _dist()
     if rank != 0:
         return 0
-    from tamc_b200 import instances as gi
-    text = gi.sa_regular(N_SPINS, DEGREE, 0)
-    betas = np.linspace(BETA0, BETA1, N_SWEEPS).astype(np.float32)
-    vals = []
-    desc, cores = "", 1
-    for i in range(args.warmup + args.steps):
-        v, desc, cores = cpu_sample(text, betas, budget_s=max(2.0, 60.0 / max(1, args.warmup + args.steps)))
-        if i >= args.warmup:
-            vals.append(v)
-    value = float(np.median(vals))
-    line = {"metric": METRIC, "value": value, "unit": "flips/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": FLIPS_PER_STEP / value * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": CONFIG,
+    if args.workload == "sa_c2":
+        rates, desc, cores = [], "", 1
+        for i in range(args.warmup + args.steps):
+            r, desc, cores = cpu_sa(max(1.0, 60.0 / max(1, args.warmup + args.steps)))
+            if i >= args.warmup:
+                rates.append(float(np.median(r)))
+        config, metric = SA_CONFIG, SA_METRIC
+    else:
+        # each step: one whole-run sample of the batch; the subset is sized so
+        # that all warm-up and timed steps end within a few minutes
+        stride = args.cpu_stride
+        t0 = time.perf_counter()
+        r, desc, cores = cpu_c3(stride, 1)
+        first = time.perf_counter() - t0
+        budget = 180.0 / max(1, args.warmup + args.steps)
+        while first > budget and stride < 64:
+            stride *= 2
+            first /= 2
+        rates = []
+        for i in range(args.warmup - 1 + args.steps):
+            r, desc, cores = cpu_c3(stride, 1)
+            if i >= args.warmup - 1:
+                rates.append(r[0])
+        desc = desc.replace("median of 1 runs in a child process", f"one run per step, median of {len(rates)} steps")
+        config, metric = C3_CONFIG, METRIC
+    value = float(np.median(rates))
+    flips = c3_flips(c3_jobs()) if args.workload != "sa_c2" else SA_FLIPS
+    line = {"metric": metric, "value": value, "unit": "flips/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": flips / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "config": config,
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "flips/s", "cores": cores, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": "flips/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -179,7 +317,8 @@ def run_reference(args):
     return 0
 
 
-def run_gpu(args):
+# ------------------------------------------------------------- GPU: C3 ----
+def run_c3(args):
     import torch
     import tamc_b200 as tb
     from tamc_b200 import instances as gi
@@ -189,26 +328,219 @@ def run_gpu(args):
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    gpu = tb.Gpu(local)
+    lib_stream = torch.cuda.ExternalStream(gpu.stream, device=dev)
+    jobs = c3_jobs(rank)
+    hosts = [tb.HostInstance.parse(gi.lattice(L, 2, "pm", si)) for L, _, si, _ in jobs]
+    params = [_lattice_params(tb, nt, C3_SWEEPS) for _, nt, _, _ in jobs]
+    dinsts = [gpu.upload(h) for h in hosts]
+    flips = c3_flips(jobs)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def make_batch(k):
+        b = tb.Batch(gpu)
+        for j, (d, p) in enumerate(zip(dinsts, params)):
+            b.add(d, p, jobs[j][3] + 7919 * k)
+        return b
+
+    def flush_l2(k):
+        with torch.cuda.stream(lib_stream):
+            flush.fill_(k & 0xFF)
+
+    for k in range(args.warmup):  # the first warm-up step also autotunes every job shape
+        b = make_batch(k)
+        b.run()
+        gpu.sync()
+        del b
+        flush_l2(k)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms, dev_ms, launches = [], 0.0, 0
+    nlaunch = 0
+    best = None
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            b = make_batch(args.warmup + k)
+            gpu.sync()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = gpu.launches
+            e0.record(lib_stream)
+            b.run()
+            e1.record(lib_stream)
+            e1.synchronize()
+            launches += gpu.launches - l0
+            step_ms.append(e0.elapsed_time(e1))
+            ms, n = b.device_time()
+            dev_ms += ms
+            nlaunch += n
+            if k == args.steps - 1:
+                best = [float(b.gs(j)[1][-1]) if len(b.gs(j)[1]) else None for j in (0, 1, 2, 3)]
+            del b
+            flush_l2(k)
+        torch.cuda.synchronize()
+    ms_total = float(np.sum(step_ms))
+    ms_t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
+    value = flips * args.steps * world / (float(ms_t.item()) / 1e3)
+
+    # end to end through the C ABI: host instances in, results out, per step
+    e2e_s, h2d, d2h = [], 0, 0
+    for k in range(max(1, min(args.steps, 3)) + 1):
+        gpu.sync()
+        c0 = tb.copy_bytes()
+        t0 = time.perf_counter()
+        di = [gpu.upload(h) for h in hosts]
+        b = tb.Batch(gpu)
+        for j, (d, p) in enumerate(zip(di, params)):
+            b.add(d, p, jobs[j][3] + 31 * k)
+        b.run()
+        res = [(b.gs(j), b.acceptance(j)) for j in range(len(jobs))]
+        del b, di
+        gpu.sync()
+        t1 = time.perf_counter()
+        c1 = tb.copy_bytes()
+        if k > 0:  # the first pass warms the host allocator and the graph cache
+            e2e_s.append(t1 - t0)
+            h2d, d2h = c1[0] - c0[0], c1[1] - c0[1]
+        assert len(res) == len(jobs)
+    e2e_t = torch.tensor([float(np.median(e2e_s))], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = flips * world / float(e2e_t.item())
+
+    out = None
+    if rank == 0:
+        clocks = clk.summary()
+        peak, kind = _peaks()
+        dev_ms_step = dev_ms / args.steps
+        bytes_step = c3_bytes(jobs)
+        achieved = bytes_step / (dev_ms_step / 1e3) / 1e9
+        traffic = _profile_value("pt_fused_c3.md", "dram_bytes_per_step")
+        inst = _profile_value("pt_fused_c3.md", "warp_instructions_per_step")
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+        issue = None
+        if inst and mhz:
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            ach, pk = inst / (dev_ms_step / 1e3), sms * 4 * mhz * 1e6
+            issue = {"achieved": ach, "peak": pk, "unit": "warp instructions/s", "frac": ach / pk,
+                     "instructions_per_step": inst, "clock_mhz": mhz,
+                     "source": "profiles/pt_fused_c3.md (smsp__inst_executed.sum over one step's chunk launches)"}
+        out = {"metric": METRIC, "value": value, "unit": "flips/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": float(ms_t.item()) / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+               "config": C3_CONFIG,
+               "flips_per_step": flips,
+               "e2e": {"value": e2e_value, "unit": "flips/s", "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(d2h),
+                       "path": "tamc_gpu_instance_upload x256, tamc_gpu_batch_create/add/run, "
+                               "tamc_gpu_batch_gs + tamc_gpu_batch_acceptance per job, destroy; wall clock",
+                       "s_per_step": float(e2e_t.item())},
+               "gpu_launches": int(launches),
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{kind} burst",
+                            "bytes_per_step": bytes_step, "kernel": "k_pt_fused (one per chunk launch)",
+                            "launch_ms_avg": dev_ms / max(1, nlaunch), "launches_per_step": nlaunch / args.steps},
+               "issue_roofline": issue,
+               "clocks": clocks, "best_energy_jobs_0_3": best}
+        if world == 1 and args.c3_plain > 0:
+            out.update(c3_plain(args, tb, gpu, lib_stream, jobs, dinsts, params, value))
+        if world == 1 and not args.no_cpu:
+            cpu = _child_json(["--cpu-leg", "c3", "--cpu-stride", str(args.cpu_stride), "--cpu-runs", "3"])
+            out["cpu_baseline"] = {"value": cpu["value"], "unit": "flips/s", "cores": cpu["cores"], "kind": "port",
+                                   "sample": cpu["sample"], "runs": cpu["runs"]}
+        elif world > 1:
+            out["cpu_baseline"] = None
+        if world == 1 and not args.no_c4:
+            out["c4"] = c4_summary(args, tb, gi, gpu)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    del gpu
+    return 0
+
+
+def c3_plain(args, tb, gpu, lib_stream, jobs, dinsts, params, batched):
+    """The plain form on jobs 0, s, 2s, ... (s = 256 / --c3-plain): one run at a
+    time, CUDA events around each run's sweep loop."""
+    import torch
+    stride = max(1, C3_JOBS // args.c3_plain)
+    sub = list(range(0, C3_JOBS, stride))
+    os.environ["TAMC_PT_FORM"] = "plain"
+    try:
+        f, ms = 0, 0.0
+        for k in sub:
+            r = tb.PtRun(dinsts[k], params[k], jobs[k][3])
+            gpu.sync()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(lib_stream)
+            r.run()
+            e1.record(lib_stream)
+            r.sync()
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            L, nt = jobs[k][0], jobs[k][1]
+            f += L * L * nt * 2 * C3_SWEEPS
+            del r
+    finally:
+        del os.environ["TAMC_PT_FORM"]
+    plain = f / (ms / 1e3)
+    return {"plain_flips_per_s": plain, "batched_over_plain": batched / plain,
+            "plain_sample": f"{len(sub)} of the 256 jobs (every {stride}th), one at a time, plain form "
+                            f"(one launch per sweep phase over all SMs), CUDA events, {f:.3g} flips in {ms / 1e3:.2f} s"}
+
+
+def c4_summary(args, tb, gi, gpu):
+    """C4 on the GPU (whole 20000-sweep run) against whole oracle runs on all cores."""
+    r = workload_pt_c4(args, tb, gi, gpu, cpu=False)
+    if not args.no_cpu:
+        cpu = _child_json(["--cpu-leg", "c4", "--c4-cpu-sweeps", str(args.c4_cpu_sweeps), "--cpu-runs", "3"])
+        r.update(cpu_flips_per_s=cpu["value"], cpu_runs=cpu["runs"], cpu_sample=cpu["sample"],
+                 cpu_cores=cpu["cores"], gpu_over_cpu=r["gpu_flips_per_s"] / cpu["value"])
+    return r
+
+
+# ------------------------------------------------------- other workloads ----
+SA_N, SA_DEG, SA_R, SA_SWEEPS = 2000, 3, 1024, 1000
+SA_FLIPS = SA_N * SA_R * SA_SWEEPS
+SA_METRIC = "spin-flip attempts/s (SA, 1 B200)"
+SA_CONFIG = {"workload": "sa_c2: N=2000 random 3-regular Ising, J~N(0,1), h~N(0,0.01), linear beta 0.1->10 x 1000 "
+                         "sweeps, 1024 restarts", "n": SA_N, "degree": SA_DEG, "restarts": SA_R, "sweeps": SA_SWEEPS,
+             "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def run_sa_c2(args):
+    """Simulated annealing, N=2000 random 3-regular, 1024 restarts x 1000 sweeps."""
+    import torch
+    import tamc_b200 as tb
+    from tamc_b200 import instances as gi
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     gpu = tb.Gpu(local)
-    text = gi.sa_regular(N_SPINS, DEGREE, 0)
-    inst = tb.HostInstance.parse(text)
-    dinst = gpu.upload(inst)
-    betas_h = np.linspace(BETA0, BETA1, N_SWEEPS).astype(np.float32)
+    dinst = gpu.upload(tb.HostInstance.parse(gi.sa_regular(SA_N, SA_DEG, 0)))
+    betas_h = np.linspace(0.1, 10.0, SA_SWEEPS).astype(np.float32)
     betas = torch.from_numpy(betas_h).to(dev)
-    energies = torch.empty(N_REPLICAS, dtype=torch.float32, device=dev)
-    words = torch.empty(((N_REPLICAS + 31) // 32) * N_SPINS, dtype=torch.int32, device=dev)
+    energies = torch.empty(SA_R, dtype=torch.float32, device=dev)
+    words = torch.empty(((SA_R + 31) // 32) * SA_N, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    # a dedicated stream: its handle is never 0, so the library launches on it
-    # and the CUDA events below time exactly those launches
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     seed0 = 1000 * (rank + 1)
 
     def step(k):
-        tb.sa_run_device(dinst, betas.data_ptr(), N_SWEEPS, N_REPLICAS, seed0 + k, energies.data_ptr(),
-                         words.data_ptr(), stream.cuda_stream)
+        tb.sa_run_device(dinst, betas.data_ptr(), SA_SWEEPS, SA_R, seed0 + k, energies.data_ptr(), words.data_ptr(),
+                         stream.cuda_stream)
 
     for k in range(args.warmup):
         step(k)
@@ -228,52 +560,36 @@ def run_gpu(args):
         torch.cuda.synchronize()
     launches = gpu.launches - launches0
     times = [a.elapsed_time(b) for a, b in evs]
-    ms = float(np.sum(times))
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    ms_t = torch.tensor([float(np.sum(times))], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = FLIPS_PER_STEP * args.steps * world / (ms_max / 1e3)
+    value = SA_FLIPS * args.steps * world / (float(ms_t.item()) / 1e3)
     e_min = float(energies.min().item())
-    # the reported quality of an anneal: best energy and the share of restarts reaching it
     frac_best = float((energies <= e_min + 1e-4 * max(1.0, abs(e_min))).float().mean().item())
-    # time to target with 99 % confidence, target = this run's best energy: one anneal
-    # of all restarts succeeds with P = 1 - (1 - frac)^restarts
-    p_anneal = 1.0 - (1.0 - frac_best) ** N_REPLICAS
-
-    # end-to-end through the C ABI with host buffers
-    reff = 0
-    t_e2e = []
-    # host buffers of the end-to-end call in pinned memory: the schedule in, energies and states out
+    p_anneal = 1.0 - (1.0 - frac_best) ** SA_R
     betas_pin = torch.from_numpy(betas_h).pin_memory().numpy()
-    e_pin = torch.empty(N_REPLICAS, dtype=torch.float32).pin_memory().numpy()
-    packed_pin = torch.empty((N_REPLICAS, (N_SPINS + 7) // 8), dtype=torch.uint8).pin_memory().numpy()
+    e_pin = torch.empty(SA_R, dtype=torch.float32).pin_memory().numpy()
+    packed_pin = torch.empty((SA_R, (SA_N + 7) // 8), dtype=torch.uint8).pin_memory().numpy()
+    t_e2e, h2d, d2h = [], 0, 0
     for k in range(max(1, min(args.steps, 5)) + 1):
         torch.cuda.synchronize()
+        c0 = tb.copy_bytes()
         t0 = time.perf_counter()
-        e_h, packed = tb.sa_run(dinst, betas_pin, N_REPLICAS, 1, seed0 + 10 ** 6 + k, tb.MODE_FAST,
-                                out=(e_pin, packed_pin))
+        tb.sa_run(dinst, betas_pin, SA_R, 1, seed0 + 10 ** 6 + k, tb.MODE_FAST, out=(e_pin, packed_pin))
         t_e2e.append(time.perf_counter() - t0)
-        reff = len(e_h)
-    e2e_s = float(np.median(t_e2e[1:]))
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        c1 = tb.copy_bytes()
+        h2d, d2h = c1[0] - c0[0], c1[1] - c0[1]
+    e2e_t = torch.tensor([float(np.median(t_e2e[1:]))], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = FLIPS_PER_STEP * world / float(e2e_t.item())
-    h2d = betas_pin.nbytes  # the instance is resident; the schedule goes in every step
-    d2h = e_pin[:reff].nbytes + packed_pin[:reff].nbytes  # energies and AnnealState bytes out
-
     out = None
     if rank == 0:
         peak, kind = _peaks()
         per_launch_ms = float(np.mean(times))
-        achieved = BYTES_PER_FLIP * FLIPS_PER_STEP / (per_launch_ms / 1e3) / 1e9
-        traffic = _profile_traffic()
+        bpf = 2 / 8 + (4 + 8 * SA_DEG + 4) / SA_R
+        achieved = bpf * SA_FLIPS / (per_launch_ms / 1e3) / 1e9
         clocks = clk.summary()
-        # The kernel keeps its state on chip, so instruction issue binds, not HBM:
-        # warp instructions per launch (ncu, same workload and tile) over the live
-        # launch time, against 4 issue slots per SM per cycle at the sampled clock.
-        inst = _profile_value("warp_instructions_per_launch")
+        inst = _profile_value("sa_fast_c2.md", "warp_instructions_per_launch")
         mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
         issue = None
         if inst and mhz:
@@ -282,40 +598,30 @@ def run_gpu(args):
             issue = {"achieved": ach, "peak": pk, "unit": "warp instructions/s", "frac": ach / pk,
                      "instructions_per_launch": inst, "clock_mhz": mhz,
                      "source": "profiles/sa_fast_c2.md (smsp__inst_executed.sum of one launch)"}
-        out = {"metric": METRIC, "value": value, "unit": "flips/s", "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        out = {"metric": SA_METRIC, "value": value, "unit": "flips/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": float(ms_t.item()) / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-               "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "1 GPU"),
-               "e2e": {"value": e2e_value, "unit": "flips/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+               "config": SA_CONFIG,
+               "e2e": {"value": SA_FLIPS * world / float(e2e_t.item()), "unit": "flips/s", "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h},
                "gpu_launches": int(launches),
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{kind} burst",
-                            "bytes_per_flip": BYTES_PER_FLIP},
-               "issue_roofline": issue,
-               "clocks": clocks, "best_energy": e_min, "restarts_at_best": frac_best,
+                            "frac": achieved / peak,
+                            "traffic": _profile_value("sa_fast_c2.md", "traffic_bytes_per_launch"),
+                            "peak_kind": f"{kind} burst", "bytes_per_flip": bpf},
+               "issue_roofline": issue, "clocks": clocks, "best_energy": e_min, "restarts_at_best": frac_best,
                "tts99_s": per_launch_ms / 1e3 * (1.0 if p_anneal >= 0.99 else
                                                 math.log(0.01) / math.log(1.0 - p_anneal))}
         if not args.no_cpu and world == 1:
-            v, desc, cores = cpu_sample(text, betas_h)
-            out["cpu_baseline"] = {"value": v, "unit": "flips/s", "cores": cores, "kind": "port", "sample": desc}
-        elif world > 1:
-            out["cpu_baseline"] = None
+            cpu = _child_json(["--cpu-leg", "sa", "--cpu-budget", "12"])
+            out["cpu_baseline"] = {"value": cpu["value"], "unit": "flips/s", "cores": cpu["cores"], "kind": "port",
+                                   "sample": cpu["sample"], "runs": cpu["runs"]}
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if out is not None:
         print(json.dumps(out), flush=True)
-    del gpu
     return 0
-
-
-# ------------------------------------------------------- other workloads ----
-# The remaining benchmark configurations, run with --workload; each prints one
-# JSON line.  They are measured separately from the headline line above.
-def _lattice_params(tb, nt, sweeps, sample=None, states=None, level=0, threads=8):
-    b = tb.geometric_betas(0.2, 5.0, nt)
-    lo = int(np.argmax(b >= np.float32(1.0))) if np.any(b >= np.float32(1.0)) else nt - 1
-    return tb.PtParams(sweeps, b, lo, 0.5, True, 2, threads, sample, states, level)
 
 
 def _time_run(tb, dinst, p, seed):
@@ -379,59 +685,13 @@ def workload_pt_c1(args, tb, gi, gpu):
     return out
 
 
-def workload_batch_c3(args, tb, gi, gpu):
-    """256 uneven 2-D +-J instances, L in {8..32}, nt in {16,24,32}, 5000 sweeps: batched vs plain."""
-    rng = np.random.default_rng(0)
-    jobs = []
-    for k in range(256):
-        L = int(rng.choice([8, 12, 16, 24, 32]))
-        nt = int(rng.choice([16, 24, 32]))
-        jobs.append((L, nt))
-    sweeps = args.c3_sweeps
-    dinsts = {}
-    batch = tb.Batch(gpu)
-    flips = 0
-    for k, (L, nt) in enumerate(jobs):
-        key = (L, k)
-        d = gpu.upload(tb.HostInstance.parse(gi.lattice(L, 2, "pm", 1000 + k)))
-        dinsts[key] = d
-        batch.add(d, _lattice_params(tb, nt, sweeps), 7 + k)
-        flips += L * L * nt * 2 * sweeps
-    import torch
-    torch.cuda.synchronize()
-    l0 = gpu.launches
-    t0 = time.perf_counter()
-    batch.run()
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    l_batch = gpu.launches - l0
-    # plain form (one instance at a time, one launch per sweep phase) on a subset
-    os.environ["TAMC_PT_FORM"] = "plain"
-    sub = list(range(0, 256, 256 // args.c3_plain)) if args.c3_plain > 0 else []
-    f_sub, t_sub = 0, 0.0
-    for k in sub:
-        L, nt = jobs[k]
-        d = dinsts[(L, k)]
-        p = _lattice_params(tb, nt, sweeps)
-        t, _ = _time_run(tb, d, p, 7 + k)
-        t_sub += t
-        f_sub += L * L * nt * 2 * sweeps
-    del os.environ["TAMC_PT_FORM"]
-    plain_rate = f_sub / t_sub if t_sub > 0 else None
-    return {"workload": "batch_c3", "instances": 256, "sweeps": sweeps, "flips": flips,
-            "batched_flips_per_s": flips / t_batch, "batched_s": t_batch, "batched_launches": int(l_batch),
-            "plain_flips_per_s": plain_rate, "plain_sample": f"{len(sub)} of 256 instances",
-            "batched_over_plain": (flips / t_batch) / plain_rate if plain_rate else None}
-
-
-def workload_pt_c4(args, tb, gi, gpu):
+def workload_pt_c4(args, tb, gi, gpu, cpu=True):
     """3-D Gaussian L=16 (N=4096), nt=64, 2 chains, ICM, 20000 sweeps, sampling every 32, suscepts."""
     L = 16
     text = gi.lattice(L, 3, "gauss", 0)
     h = tb.HostInstance.parse(text)
-    w = [gi.fourier_weights(L, 3, 0), gi.fourier_weights(L, 3, 1)]
-    for row in w:
-        h.add_suscept(row)
+    for ax in (0, 1):
+        h.add_suscept(gi.fourier_weights(L, 3, ax))
     d = gpu.upload(h)
     sweeps = args.c4_sweeps
     p = _lattice_params(tb, 64, sweeps, 32, 32, 0, threads=64)
@@ -440,26 +700,19 @@ def workload_pt_c4(args, tb, gi, gpu):
     t_gpu, r = _time_run(tb, d, p, 2)
     best = float(r.gs()[1][-1])
     first, tts = _time_to_target(tb, d, p, 2, best, t_gpu / sweeps)
-    out = {"workload": "pt_c4", "sweeps": sweeps, "flips": flips, "gpu_flips_per_s": flips / t_gpu, "gpu_s": t_gpu,
-           "gpu_best_energy": best, "target_energy": best, "target_first_sweep": first, "time_to_target_s": tts}
-    if not args.no_cpu:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import pyoracle as po
-        inst = po.Instance.from_text(text)
-        for row in w:
-            inst.add_suscept(row)
-        k = args.c4_cpu_sweeps
-        cores = os.cpu_count() or 1
-        orc = po.PtRun(inst, p.betas, k, 0.0, p.lo_beta_idx, True, 2, 64, sample=32, sample_states=32,
-                       sample_limiting=0, seed=3)
-        t0 = time.perf_counter()
-        orc.run(nthreads=cores)
-        t_cpu = time.perf_counter() - t0
-        cpu_rate = 4096 * 64 * 2 * k / t_cpu
-        out.update(cpu_flips_per_s=cpu_rate, cpu_sample=f"oracle run_parallel (threads: 64), first {k} sweeps "
-                   f"measured every sweep, {cores} OpenMP threads", cpu_cores=cores,
-                   gpu_over_cpu=(flips / t_gpu) / cpu_rate)
+    out = {"workload": "pt_c4: 3-D L=16 Gaussian, 64 temperatures, 2 chains, ICM, samples every 32",
+           "sweeps": sweeps, "flips": flips, "gpu_flips_per_s": flips / t_gpu, "gpu_s": t_gpu,
+           "gpu_best_energy": best, "target_energy": best,
+           "target_first_sweep": first, "time_to_target_s": tts}
+    if cpu and not args.no_cpu:
+        c = _child_json(["--cpu-leg", "c4", "--c4-cpu-sweeps", str(args.c4_cpu_sweeps), "--cpu-runs", "3"])
+        out.update(cpu_flips_per_s=c["value"], cpu_runs=c["runs"], cpu_sample=c["sample"], cpu_cores=c["cores"],
+                   gpu_over_cpu=(flips / t_gpu) / c["value"])
     return out
+
+
+def workload_batch_c3(args, tb, gi, gpu):
+    raise SystemExit("batch_c3 is the default line: run bench.py without --workload")
 
 
 def workload_serve_c5(args, tb, gi, gpu):
@@ -506,8 +759,7 @@ def run_workload(args):
     from tamc_b200 import instances as gi
     torch.cuda.set_device(0)
     gpu = tb.Gpu(0)
-    fn = {"pt_c1": workload_pt_c1, "batch_c3": workload_batch_c3, "pt_c4": workload_pt_c4,
-          "serve_c5": workload_serve_c5}[args.workload]
+    fn = {"pt_c1": workload_pt_c1, "pt_c4": workload_pt_c4, "serve_c5": workload_serve_c5}[args.workload]
     with ClockSampler(0) as clk:
         out = fn(args, tb, gi, gpu)
     out["metric"] = "spin-flip attempts/s"
@@ -522,22 +774,30 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="sa_c2", choices=["sa_c2", "pt_c1", "batch_c3", "pt_c4", "serve_c5"])
-    ap.add_argument("--c3-sweeps", type=int, default=5000)
-    ap.add_argument("--c3-plain", type=int, default=16, help="instances of the plain-form comparison (0 skips it)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline legs")
+    ap.add_argument("--no-c4", action="store_true", help="skip the C4 keys of the default line")
+    ap.add_argument("--workload", default="batch_c3", choices=["batch_c3", "sa_c2", "pt_c1", "pt_c4", "serve_c5"])
+    ap.add_argument("--c3-plain", type=int, default=64, help="jobs of the plain-form comparison (0 skips it)")
     ap.add_argument("--c4-sweeps", type=int, default=20000)
-    ap.add_argument("--c4-cpu-sweeps", type=int, default=200)
+    ap.add_argument("--c4-cpu-sweeps", type=int, default=1000)
     ap.add_argument("--c5-requests", type=int, default=1000)
     ap.add_argument("--c5-rate", type=float, default=100.0)
+    ap.add_argument("--cpu-leg", choices=["c3", "c4", "sa"], help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-stride", type=int, default=8, help="C3 CPU sample: every k-th job")
+    ap.add_argument("--cpu-runs", type=int, default=3)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
     args = ap.parse_args()
+    if args.cpu_leg:
+        return run_cpu_leg(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload != "sa_c2":
-        return run_workload(args)
-    return run_gpu(args)
+    if args.workload == "batch_c3":
+        return run_c3(args)
+    if args.workload == "sa_c2":
+        return run_sa_c2(args)
+    return run_workload(args)
 
 
 if __name__ == "__main__":

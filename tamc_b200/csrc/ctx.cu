@@ -9,6 +9,8 @@ extern "C" const unsigned char tamc_expf_blob_end[];
 
 namespace tamc {
 
+std::atomic<uint64_t> g_h2d_bytes{0}, g_d2h_bytes{0};
+
 static inline uint64_t sm64(uint64_t& st) {
   st += 0x9e3779b97f4a7c15ULL;
   uint64_t z = st;
@@ -53,7 +55,7 @@ static T* dmalloc_copy(const T* h, size_t count) {
   T* d = nullptr;
   const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
   TAMC_CUDA(cudaMalloc((void**)&d, bytes));
-  if (count) TAMC_CUDA(cudaMemcpy(d, h, count * sizeof(T), cudaMemcpyHostToDevice));
+  if (count) TAMC_CUDA(copy_sync(d, h, count * sizeof(T), cudaMemcpyHostToDevice));
   return d;
 }
 
@@ -143,6 +145,11 @@ float tamc_ref_expf(float x) {
   const uint32_t nb = blob[1], ne = blob[2];
   const uint32_t* off = blob + 3;
   return tamc_expf_exact(x, off, off + nb + 1, off + nb + 1 + ne);
+}
+
+void tamc_copy_bytes(uint64_t* h2d, uint64_t* d2h) {
+  if (h2d) *h2d = g_h2d_bytes.load();
+  if (d2h) *d2h = g_d2h_bytes.load();
 }
 
 void* tamc_gpu_stream(tamc_gpu* g) { return g ? (void*)g->stream : nullptr; }

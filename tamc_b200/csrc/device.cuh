@@ -19,6 +19,24 @@ namespace tamc {
       ::tamc::fail(TAMC_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
   } while (0)
 
+// Bytes this library has copied between host and device (all contexts, since
+// load), by direction; reported through tamc_copy_bytes.  Every host<->device
+// copy goes through copy_async / copy_sync, or calls count_copy where a
+// captured graph replays a copy.
+extern std::atomic<uint64_t> g_h2d_bytes, g_d2h_bytes;
+inline void count_copy(size_t bytes, cudaMemcpyKind kind) {
+  if (kind == cudaMemcpyHostToDevice) g_h2d_bytes.fetch_add(bytes, std::memory_order_relaxed);
+  else if (kind == cudaMemcpyDeviceToHost) g_d2h_bytes.fetch_add(bytes, std::memory_order_relaxed);
+}
+inline cudaError_t copy_async(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
+  count_copy(bytes, kind);
+  return cudaMemcpyAsync(dst, src, bytes, kind, st);
+}
+inline cudaError_t copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+  count_copy(bytes, kind);
+  return cudaMemcpy(dst, src, bytes, kind);
+}
+
 // ------------------------------------------------------------ RNG ----
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of the
 // multiply-hi/lo Feistel round with multipliers 0xD2511F53 / 0xCD9E8D57 and

@@ -106,7 +106,7 @@ static float time_tile(tamc_gpu* g, const PtJob& proto, TileChoice t, uint32_t r
     j.init = rep == 0 ? 1 : 0;
     j.sweep_begin = rep * rounds;
     j.sweep_end = (rep + 1) * rounds;
-    TAMC_CUDA(cudaMemcpyAsync(dj.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
+    TAMC_CUDA(tamc::copy_async(dj.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
     ctr.zero(st);
     TAMC_CUDA(cudaEventRecord(e0, st));
     fused_launch(st, dj.p, 1, ctr.p, 1, t.T, smem);
@@ -191,13 +191,13 @@ static void fill_job(tamc_pt* pt, uint64_t seed, tamc_pt::FastState* F) {
   F->ctr.alloc(1);
   std::vector<float> b(j.ntp, 0.0f);
   std::copy(c.betas.begin(), c.betas.end(), b.begin());
-  TAMC_CUDA(cudaMemcpyAsync(F->betas.p, b.data(), j.ntp * 4, cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(F->betas.p, b.data(), j.ntp * 4, cudaMemcpyHostToDevice, st));
   std::vector<uint8_t> tags((size_t)j.C * j.nt, 0);
   for (uint32_t ch = 0; ch < j.C; ++ch) {
     tags[(size_t)ch * j.nt] = 1;
     tags[(size_t)ch * j.nt + j.nt - 1] = 2;
   }
-  TAMC_CUDA(cudaMemcpyAsync(F->tags.p, tags.data(), tags.size(), cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(F->tags.p, tags.data(), tags.size(), cudaMemcpyHostToDevice, st));
   F->acc.zero(st);
   F->rtrips.zero(st);
   F->dhist.zero(st);
@@ -260,7 +260,7 @@ static void launch_one(tamc_pt* pt, uint32_t begin, uint32_t end, int init) {
   j.sweep_end = end;
   j.m_base = pt->m_next;
   j.s_base = pt->s_next;
-  TAMC_CUDA(cudaMemcpyAsync(F->d_job.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(F->d_job.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
   F->ctr.zero(st);
   fused_launch(st, F->d_job.p, 1, F->ctr.p, 1, F->T, F->smem);
   pt->g->count();
@@ -324,7 +324,7 @@ static void plain_setup(tamc_pt* pt) {
   if (plain_icm_bytes(j) > pt->g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the plain ICM kernel");
   j.init = 0;
   j.count_out = nullptr;
-  TAMC_CUDA(cudaMemcpyAsync(F->d_job.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(F->d_job.p, &j, sizeof(PtJob), cudaMemcpyHostToDevice, st));
 }
 
 static void plain_init_energies(tamc_pt* pt, bool random) {
@@ -437,8 +437,8 @@ void fast_pt_get_state(tamc_pt* pt, int8_t* spins, float* energies) {
   cudaStream_t st = pt->g->stream;
   std::vector<uint32_t> W((size_t)j.n * j.nw);
   std::vector<double> Ec((size_t)j.C * j.ntp);
-  TAMC_CUDA(cudaMemcpyAsync(W.data(), F->W.p, W.size() * 4, cudaMemcpyDeviceToHost, st));
-  TAMC_CUDA(cudaMemcpyAsync(Ec.data(), F->Ec.p, Ec.size() * 8, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(tamc::copy_async(W.data(), F->W.p, W.size() * 4, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(tamc::copy_async(Ec.data(), F->Ec.p, Ec.size() * 8, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
   const std::vector<uint32_t>& perm = pt->inst->h_perm;
   for (uint32_t ch = 0; ch < j.C; ++ch)
@@ -464,23 +464,23 @@ void fast_pt_set_state(tamc_pt* pt, const int8_t* spins) {
       for (uint32_t s = 0; s < j.n; ++s)
         if (src[perm[s]] < 0) W[(size_t)s * j.nw + o] |= 1u << b;
     }
-  TAMC_CUDA(cudaMemcpyAsync(F->W.p, W.data(), W.size() * 4, cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(F->W.p, W.data(), W.size() * 4, cudaMemcpyHostToDevice, st));
   if (F->plain) plain_init_energies(pt, false);
   else launch_one(pt, pt->next_sweep, pt->next_sweep, 2);  // recompute energies
 }
 
 void fast_pt_acceptance(tamc_pt* pt, uint32_t* acc) {
   auto* F = pt->fast;
-  TAMC_CUDA(cudaMemcpyAsync(acc, F->acc.p, F->acc.n * 4, cudaMemcpyDeviceToHost, pt->g->stream));
+  TAMC_CUDA(tamc::copy_async(acc, F->acc.p, F->acc.n * 4, cudaMemcpyDeviceToHost, pt->g->stream));
   TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
 }
 
 void fast_pt_round_trips(tamc_pt* pt, uint8_t* tags, uint32_t* round_trips, uint32_t* dhist) {
   auto* F = pt->fast;
   cudaStream_t st = pt->g->stream;
-  if (tags) TAMC_CUDA(cudaMemcpyAsync(tags, F->tags.p, F->tags.n, cudaMemcpyDeviceToHost, st));
-  if (round_trips) TAMC_CUDA(cudaMemcpyAsync(round_trips, F->rtrips.p, F->rtrips.n * 4, cudaMemcpyDeviceToHost, st));
-  if (dhist) TAMC_CUDA(cudaMemcpyAsync(dhist, F->dhist.p, F->dhist.n * 4, cudaMemcpyDeviceToHost, st));
+  if (tags) TAMC_CUDA(tamc::copy_async(tags, F->tags.p, F->tags.n, cudaMemcpyDeviceToHost, st));
+  if (round_trips) TAMC_CUDA(tamc::copy_async(round_trips, F->rtrips.p, F->rtrips.n * 4, cudaMemcpyDeviceToHost, st));
+  if (dhist) TAMC_CUDA(tamc::copy_async(dhist, F->dhist.p, F->dhist.n * 4, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -488,7 +488,7 @@ void fast_pt_phase_cycles(tamc_pt* pt, uint64_t* out) {
   auto* F = pt->fast;
   for (int k = 0; k < PHASE_N; ++k) out[k] = 0;
   if (!F || !F->prof.p) return;
-  TAMC_CUDA(cudaMemcpyAsync(out, F->prof.p, PHASE_N * 8, cudaMemcpyDeviceToHost, pt->g->stream));
+  TAMC_CUDA(tamc::copy_async(out, F->prof.p, PHASE_N * 8, cudaMemcpyDeviceToHost, pt->g->stream));
   TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
 }
 
@@ -517,7 +517,16 @@ struct ChunkRunner {
   cudaGraphExec_t exec = nullptr;
   uint32_t g_n = 0, g_grid = 0, g_T = 0;
   size_t g_smem = 0;
-  ~ChunkRunner() { reset(); }
+  // device time of the chunk launches (CUDA events around each one: the job
+  // table upload, the fused kernel and the count readback) and their number
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double dev_ms = 0.0;
+  uint64_t launches = 0;
+  ~ChunkRunner() {
+    reset();
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
   void reset() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -533,6 +542,8 @@ struct ChunkRunner {
     if (n <= cap_jobs) return;
     reset();
     cap_jobs = std::max(n, 16u);
+    for (auto& e : ev)
+      if (!e) TAMC_CUDA(cudaEventCreate(&e));
     TAMC_CUDA(cudaMallocHost((void**)&h_jobs, cap_jobs * sizeof(PtJob)));
     TAMC_CUDA(cudaMallocHost((void**)&h_counts, cap_jobs * sizeof(uint32_t)));
     d_jobs.alloc(cap_jobs);
@@ -609,6 +620,7 @@ struct ChunkRunner {
         exec = nullptr;
         graph = nullptr;
         TAMC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        // the graph's two copies are counted at every replay below
         cudaMemcpyAsync(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st);
         cudaMemsetAsync(ctr.p, 0, 4, st);
         fused_launch(st, d_jobs.p, na, ctr.p, grid, T, smem);
@@ -620,15 +632,25 @@ struct ChunkRunner {
         g_T = T;
         g_smem = smem;
       }
+      TAMC_CUDA(cudaEventRecord(ev[0], st));
       TAMC_CUDA(cudaGraphLaunch(exec, st));
+      TAMC_CUDA(cudaEventRecord(ev[1], st));
+      count_copy(na * sizeof(PtJob), cudaMemcpyHostToDevice);
+      count_copy(na * 4, cudaMemcpyDeviceToHost);
     } else {
-      TAMC_CUDA(cudaMemcpyAsync(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st));
+      TAMC_CUDA(cudaEventRecord(ev[0], st));
+      TAMC_CUDA(tamc::copy_async(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st));
       TAMC_CUDA(cudaMemsetAsync(ctr.p, 0, 4, st));
       fused_launch(st, d_jobs.p, na, ctr.p, grid, T, smem);
-      TAMC_CUDA(cudaMemcpyAsync(h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st));
+      TAMC_CUDA(tamc::copy_async(h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st));
+      TAMC_CUDA(cudaEventRecord(ev[1], st));
     }
     g->count();
     TAMC_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.0f;
+    TAMC_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    dev_ms += ms;
+    ++launches;
     for (uint32_t x = 0; x < na; ++x) {
       tamc_pt* pt = act[x];
       const PtCfg& c = pt->cfg;
@@ -715,6 +737,17 @@ int tamc_gpu_batch_get_state(tamc_batch* b, uint32_t job, int8_t* spins, float* 
   return tamc_gpu_pt_get_state(job_of(b, job), spins, energies);
   TAMC_API_END
 }
+int tamc_gpu_batch_set_state(tamc_batch* b, uint32_t job, const int8_t* spins) {
+  TAMC_API_BEGIN
+  return tamc_gpu_pt_set_state(job_of(b, job), spins);
+  TAMC_API_END
+}
+int tamc_gpu_batch_round_trips(tamc_batch* b, uint32_t job, uint8_t* tags, uint32_t* round_trips,
+                               uint32_t* diffusion_hist) {
+  TAMC_API_BEGIN
+  return tamc_gpu_pt_round_trips(job_of(b, job), tags, round_trips, diffusion_hist);
+  TAMC_API_END
+}
 int tamc_gpu_batch_acceptance(tamc_batch* b, uint32_t job, uint32_t* counts) {
   TAMC_API_BEGIN
   return tamc_gpu_pt_acceptance(job_of(b, job), counts);
@@ -734,6 +767,13 @@ int tamc_gpu_batch_samples_dims(tamc_batch* b, uint32_t job, uint32_t* M, uint32
 int tamc_gpu_batch_samples(tamc_batch* b, uint32_t job, float* e, int32_t* q, float* suscept, uint8_t* samples) {
   TAMC_API_BEGIN
   return tamc_gpu_pt_samples(job_of(b, job), e, q, suscept, samples);
+  TAMC_API_END
+}
+int tamc_gpu_batch_device_time(tamc_batch* b, double* ms, uint64_t* launches) {
+  TAMC_API_BEGIN
+  if (!b) fail(TAMC_E_INVAL, "null batch");
+  if (ms) *ms = b->runner.dev_ms;
+  if (launches) *launches = b->runner.launches;
   TAMC_API_END
 }
 int tamc_gpu_batch_tile(tamc_batch* b, uint32_t job, uint32_t* cta_threads, uint32_t* slots_per_task, int32_t* csr_in_smem) {

@@ -211,7 +211,7 @@ SaTile sa_fast_choose(tamc_gpu* g, const FastInst& F, uint32_t R) {
     TAMC_CUDA(cudaMalloc((void**)&d_w, (size_t)((R + 31) / 32) * F.n * 4));
     std::vector<float> hb(nb);
     for (uint32_t k = 0; k < nb; ++k) hb[k] = 0.1f + 9.9f * (float)k / (float)(nb - 1);  // an annealing ramp
-    TAMC_CUDA(cudaMemcpy(d_b, hb.data(), nb * 4, cudaMemcpyHostToDevice));
+    TAMC_CUDA(copy_sync(d_b, hb.data(), nb * 4, cudaMemcpyHostToDevice));
     cudaEvent_t e0, e1;
     TAMC_CUDA(cudaEventCreate(&e0));
     TAMC_CUDA(cudaEventCreate(&e1));

@@ -92,7 +92,7 @@ GsLog PtOutputs::log() const {
 
 void PtOutputs::drain(cudaStream_t st) {
   uint32_t cnt = 0;
-  TAMC_CUDA(cudaMemcpyAsync(&cnt, gs_count.p, 4, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(tamc::copy_async(&cnt, gs_count.p, 4, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
   if (cnt > cap) fail(TAMC_E_INVAL, "ground-state log overflow");
   if (cnt) {
@@ -101,23 +101,22 @@ void PtOutputs::drain(cudaStream_t st) {
     h_steps.resize(b + cnt);
     h_E.resize(b + cnt);
     h_words.resize((b + cnt) * nw);
-    TAMC_CUDA(cudaMemcpyAsync(h_steps.data() + b, gs_steps.p, cnt * 4, cudaMemcpyDeviceToHost, st));
-    TAMC_CUDA(cudaMemcpyAsync(h_E.data() + b, gs_E.p, cnt * 4, cudaMemcpyDeviceToHost, st));
-    TAMC_CUDA(cudaMemcpyAsync(h_words.data() + b * nw, gs_words.p, cnt * nw * 8, cudaMemcpyDeviceToHost, st));
+    TAMC_CUDA(tamc::copy_async(h_steps.data() + b, gs_steps.p, cnt * 4, cudaMemcpyDeviceToHost, st));
+    TAMC_CUDA(tamc::copy_async(h_E.data() + b, gs_E.p, cnt * 4, cudaMemcpyDeviceToHost, st));
+    TAMC_CUDA(tamc::copy_async(h_words.data() + b * nw, gs_words.p, cnt * nw * 8, cudaMemcpyDeviceToHost, st));
     TAMC_CUDA(cudaMemsetAsync(gs_count.p, 0, 4, st));
     TAMC_CUDA(cudaStreamSynchronize(st));
   }
   pending = 0;
 }
 
-static void ref_create(tamc_pt* pt, uint64_t seed) {
+static void ref_create(tamc_pt* pt, Xo master) {
   const PtCfg& c = pt->cfg;
   tamc_inst* I = pt->inst;
   cudaStream_t st = pt->g->stream;
   const uint32_t n = I->n, R = c.C * c.nt;
   // generate_init_state (src/pt.rs:506-519): chains outer, temperatures inner,
   // n draws each from the master stream.
-  Xo master = xo_seed_from_u64(seed);
   std::vector<int8_t> h((size_t)R * n);
   for (uint32_t r = 0; r < R; ++r)
     for (uint32_t i = 0; i < n; ++i) h[(size_t)r * n + i] = (master.next_u32() >> 31) ? 1 : -1;
@@ -155,12 +154,12 @@ static void ref_create(tamc_pt* pt, uint64_t seed) {
   }
   std::vector<float> db(c.nt, 0.0f);
   for (uint32_t k = 0; k + 1 < c.nt; ++k) db[k] = c.betas[k + 1] - c.betas[k];
-  TAMC_CUDA(cudaMemcpyAsync(pt->spins.p, h.data(), h.size(), cudaMemcpyHostToDevice, st));
-  TAMC_CUDA(cudaMemcpyAsync(pt->perm.p, perm.data(), R * 4, cudaMemcpyHostToDevice, st));
-  TAMC_CUDA(cudaMemcpyAsync(pt->tags.p, tags.data(), R, cudaMemcpyHostToDevice, st));
-  TAMC_CUDA(cudaMemcpyAsync(pt->d_betas.p, c.betas.data(), c.nt * 4, cudaMemcpyHostToDevice, st));
-  TAMC_CUDA(cudaMemcpyAsync(pt->d_dbeta.p, db.data(), c.nt * 4, cudaMemcpyHostToDevice, st));
-  TAMC_CUDA(cudaMemcpyAsync(pt->rng.p, rv.data(), rv.size() * sizeof(Xo), cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(pt->spins.p, h.data(), h.size(), cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(pt->perm.p, perm.data(), R * 4, cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(pt->tags.p, tags.data(), R, cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(pt->d_betas.p, c.betas.data(), c.nt * 4, cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(pt->d_dbeta.p, db.data(), c.nt * 4, cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(pt->rng.p, rv.data(), rv.size() * sizeof(Xo), cudaMemcpyHostToDevice, st));
   pt->acc.zero(st);
   pt->rtrips.zero(st);
   pt->dhist.zero(st);
@@ -194,7 +193,7 @@ static RefPt ref_view(tamc_pt* pt) {
 static void check_err(tamc_pt* pt) {
   if (!pt->err.p) return;
   int e = 0;
-  TAMC_CUDA(cudaMemcpyAsync(&e, pt->err.p, 4, cudaMemcpyDeviceToHost, pt->g->stream));
+  TAMC_CUDA(tamc::copy_async(&e, pt->err.p, 4, cudaMemcpyDeviceToHost, pt->g->stream));
   TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
   if (e == TAMC_E_REFPANIC) fail(TAMC_E_REFPANIC, "ICM seed site outside the coupling graph (the reference panics)");
   if (e) fail(e, "device error");
@@ -232,6 +231,27 @@ static void ref_round(tamc_pt* pt, uint32_t i) {
   TAMC_CUDA(cudaGetLastError());
 }
 
+tamc_pt* pt_create_ref_stream(tamc_inst* inst, const tamc_pt_params* p, const Xo& master) {
+  if (!inst || !p) fail(TAMC_E_INVAL, "null argument");
+  TAMC_CUDA(cudaSetDevice(inst->g->device));
+  auto* pt = new tamc_pt();
+  tamc_inst_retain(inst);
+  try {
+    pt->inst = inst;
+    pt->g = inst->g;
+    pt->mode = TAMC_MODE_REF;
+    pt->cfg = make_cfg(p);
+    pt->out.init(pt->cfg, inst->n, inst->nchi, pt->g->stream);
+    ref_create(pt, master);
+    TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
+  } catch (...) {
+    delete pt;
+    tamc_inst_release(inst);
+    throw;
+  }
+  return pt;
+}
+
 }  // namespace tamc
 
 using namespace tamc;
@@ -251,7 +271,7 @@ int tamc_gpu_pt_create(tamc_inst* inst, const tamc_pt_params* p, uint64_t seed, 
     pt->mode = mode;
     pt->cfg = make_cfg(p);
     pt->out.init(pt->cfg, inst->n, inst->nchi, pt->g->stream);
-    if (mode == TAMC_MODE_REF) ref_create(pt, seed);
+    if (mode == TAMC_MODE_REF) ref_create(pt, xo_seed_from_u64(seed));
     else fast_pt_create(pt, seed);
     TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
   } catch (...) {
@@ -317,9 +337,9 @@ int tamc_gpu_pt_get_state(tamc_pt* pt, int8_t* spins, float* energies) {
   std::vector<int8_t> h((size_t)R * n);
   std::vector<float> e(R);
   std::vector<uint32_t> perm(R);
-  TAMC_CUDA(cudaMemcpyAsync(h.data(), pt->spins.p, h.size(), cudaMemcpyDeviceToHost, st));
-  TAMC_CUDA(cudaMemcpyAsync(e.data(), pt->energy.p, R * 4, cudaMemcpyDeviceToHost, st));
-  TAMC_CUDA(cudaMemcpyAsync(perm.data(), pt->perm.p, R * 4, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(tamc::copy_async(h.data(), pt->spins.p, h.size(), cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(tamc::copy_async(e.data(), pt->energy.p, R * 4, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(tamc::copy_async(perm.data(), pt->perm.p, R * 4, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
   for (uint32_t k = 0; k < R; ++k) {
     if (spins) memcpy(spins + (size_t)k * n, h.data() + (size_t)perm[k] * n, n);
@@ -342,11 +362,11 @@ int tamc_gpu_pt_set_state(tamc_pt* pt, const int8_t* spins) {
   }
   cudaStream_t st = pt->g->stream;
   std::vector<uint32_t> perm(R);
-  TAMC_CUDA(cudaMemcpyAsync(perm.data(), pt->perm.p, R * 4, cudaMemcpyDeviceToHost, st));
+  TAMC_CUDA(tamc::copy_async(perm.data(), pt->perm.p, R * 4, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
   std::vector<int8_t> h((size_t)R * n);
   for (uint32_t k = 0; k < R; ++k) memcpy(h.data() + (size_t)perm[k] * n, spins + (size_t)k * n, n);
-  TAMC_CUDA(cudaMemcpyAsync(pt->spins.p, h.data(), h.size(), cudaMemcpyHostToDevice, st));
+  TAMC_CUDA(tamc::copy_async(pt->spins.p, h.data(), h.size(), cudaMemcpyHostToDevice, st));
   ref_energy_all(st, make_ref_inst(pt->inst), pt->spins.p, pt->energy.p, R);
   pt->g->count();
   TAMC_CUDA(cudaStreamSynchronize(st));
@@ -362,7 +382,7 @@ int tamc_gpu_pt_acceptance(tamc_pt* pt, uint32_t* counts) {
   if (pt->mode == TAMC_MODE_FAST) {
     fast_pt_acceptance(pt, acc.data());
   } else {
-    TAMC_CUDA(cudaMemcpyAsync(acc.data(), pt->acc.p, acc.size() * 4, cudaMemcpyDeviceToHost, pt->g->stream));
+    TAMC_CUDA(tamc::copy_async(acc.data(), pt->acc.p, acc.size() * 4, cudaMemcpyDeviceToHost, pt->g->stream));
     TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
   }
   for (uint32_t t = 0; t < c.nt; ++t) {
@@ -383,10 +403,10 @@ int tamc_gpu_pt_round_trips(tamc_pt* pt, uint8_t* tags, uint32_t* round_trips, u
     return TAMC_OK;
   }
   cudaStream_t st = pt->g->stream;
-  if (tags) TAMC_CUDA(cudaMemcpyAsync(tags, pt->tags.p, (size_t)c.C * c.nt, cudaMemcpyDeviceToHost, st));
-  if (round_trips) TAMC_CUDA(cudaMemcpyAsync(round_trips, pt->rtrips.p, c.C * 4, cudaMemcpyDeviceToHost, st));
+  if (tags) TAMC_CUDA(tamc::copy_async(tags, pt->tags.p, (size_t)c.C * c.nt, cudaMemcpyDeviceToHost, st));
+  if (round_trips) TAMC_CUDA(tamc::copy_async(round_trips, pt->rtrips.p, c.C * 4, cudaMemcpyDeviceToHost, st));
   if (diffusion_hist)
-    TAMC_CUDA(cudaMemcpyAsync(diffusion_hist, pt->dhist.p, (size_t)c.C * c.nt * 8, cudaMemcpyDeviceToHost, st));
+    TAMC_CUDA(tamc::copy_async(diffusion_hist, pt->dhist.p, (size_t)c.C * c.nt * 8, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
   TAMC_API_END
 }
@@ -422,10 +442,10 @@ int tamc_gpu_pt_samples(tamc_pt* pt, float* e, int32_t* q, float* suscept, uint8
   TAMC_CUDA(cudaSetDevice(pt->g->device));
   cudaStream_t st = pt->g->stream;
   const PtOutputs& o = pt->out;
-  if (e) TAMC_CUDA(cudaMemcpyAsync(e, o.e.p, o.e.n * 4, cudaMemcpyDeviceToHost, st));
-  if (q) TAMC_CUDA(cudaMemcpyAsync(q, o.q.p, o.q.n * 4, cudaMemcpyDeviceToHost, st));
-  if (suscept) TAMC_CUDA(cudaMemcpyAsync(suscept, o.sus.p, o.sus.n * 4, cudaMemcpyDeviceToHost, st));
-  if (samples) TAMC_CUDA(cudaMemcpyAsync(samples, o.samp.p, o.samp.n, cudaMemcpyDeviceToHost, st));
+  if (e) TAMC_CUDA(tamc::copy_async(e, o.e.p, o.e.n * 4, cudaMemcpyDeviceToHost, st));
+  if (q) TAMC_CUDA(tamc::copy_async(q, o.q.p, o.q.n * 4, cudaMemcpyDeviceToHost, st));
+  if (suscept) TAMC_CUDA(tamc::copy_async(suscept, o.sus.p, o.sus.n * 4, cudaMemcpyDeviceToHost, st));
+  if (samples) TAMC_CUDA(tamc::copy_async(samples, o.samp.p, o.samp.n, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
   TAMC_API_END
 }

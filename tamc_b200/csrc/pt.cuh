@@ -76,6 +76,13 @@ struct PtOutputs {
 
 }  // namespace tamc
 
+namespace tamc {
+// A reference-order run whose initial replicas and serial loop draw from the
+// Xoshiro256++ state `master` (p->threads should be <= 1: the single-stream
+// pt_loop), as GLA's sub-solvers run (src/gla.rs:148-166).
+tamc_pt* pt_create_ref_stream(tamc_inst* inst, const tamc_pt_params* p, const Xo& master);
+}  // namespace tamc
+
 struct tamc_pt {
   tamc_inst* inst = nullptr;
   tamc_gpu* g = nullptr;

@@ -76,7 +76,7 @@ int tamc_gpu_sa_run(tamc_inst* inst, const float* betas, uint32_t nbeta, uint32_
     SaScratch& sc = inst->sa_scratch;
     const uint32_t nw = (R + 31) / 32;
     sc.ensure((size_t)nw * n, R, (size_t)R * nbytes, nbeta);
-    if (nbeta) TAMC_CUDA(cudaMemcpyAsync(sc.betas, betas, nbeta * 4, cudaMemcpyHostToDevice, st));
+    if (nbeta) TAMC_CUDA(tamc::copy_async(sc.betas, betas, nbeta * 4, cudaMemcpyHostToDevice, st));
     TAMC_CUDA(cudaMemsetAsync(sc.words, 0, (size_t)nw * n * 4, st));
     SaFastArgs a;
     a.F = make_fast_inst(inst);
@@ -91,14 +91,14 @@ int tamc_gpu_sa_run(tamc_inst* inst, const float* betas, uint32_t nbeta, uint32_
     sa_fast_launch(st, a, t);
     sa_pack_states(st, sc.words, n, R, sc.packed);
     g->count(2);
-    if (energies_out) TAMC_CUDA(cudaMemcpyAsync(energies_out, sc.energies, R * 4, cudaMemcpyDeviceToHost, st));
+    if (energies_out) TAMC_CUDA(tamc::copy_async(energies_out, sc.energies, R * 4, cudaMemcpyDeviceToHost, st));
     if (packed_out)
-      TAMC_CUDA(cudaMemcpyAsync(packed_out, sc.packed, (size_t)R * nbytes, cudaMemcpyDeviceToHost, st));
+      TAMC_CUDA(tamc::copy_async(packed_out, sc.packed, (size_t)R * nbytes, cudaMemcpyDeviceToHost, st));
     TAMC_CUDA(cudaStreamSynchronize(st));
     return TAMC_OK;
   }
   DBuf<float> d_betas(nbeta);
-  if (nbeta) TAMC_CUDA(cudaMemcpyAsync(d_betas.p, betas, nbeta * 4, cudaMemcpyHostToDevice, st));
+  if (nbeta) TAMC_CUDA(tamc::copy_async(d_betas.p, betas, nbeta * 4, cudaMemcpyHostToDevice, st));
   std::vector<float> e(R);
   std::vector<uint8_t> packed((size_t)R * nbytes, 0);
   if (mode == TAMC_MODE_REF) {
@@ -119,15 +119,15 @@ int tamc_gpu_sa_run(tamc_inst* inst, const float* betas, uint32_t nbeta, uint32_
     DBuf<int8_t> d_spins((size_t)R * n);
     DBuf<Xo> d_rng(parts);
     DBuf<float> d_e(R);
-    TAMC_CUDA(cudaMemcpyAsync(d_spins.p, spins.data(), spins.size(), cudaMemcpyHostToDevice, st));
-    TAMC_CUDA(cudaMemcpyAsync(d_rng.p, rv.data(), parts * sizeof(Xo), cudaMemcpyHostToDevice, st));
+    TAMC_CUDA(tamc::copy_async(d_spins.p, spins.data(), spins.size(), cudaMemcpyHostToDevice, st));
+    TAMC_CUDA(tamc::copy_async(d_rng.p, rv.data(), parts * sizeof(Xo), cudaMemcpyHostToDevice, st));
     const RefInst I = make_ref_inst(inst);
     ref_sa(st, I, g->exp, d_spins.p, d_rng.p, parts, per, d_betas.p, nbeta);
     ref_energy_all(st, I, d_spins.p, d_e.p, R);
     g->count(2);
     TAMC_CUDA(cudaGetLastError());
-    TAMC_CUDA(cudaMemcpyAsync(spins.data(), d_spins.p, spins.size(), cudaMemcpyDeviceToHost, st));
-    TAMC_CUDA(cudaMemcpyAsync(e.data(), d_e.p, R * 4, cudaMemcpyDeviceToHost, st));
+    TAMC_CUDA(tamc::copy_async(spins.data(), d_spins.p, spins.size(), cudaMemcpyDeviceToHost, st));
+    TAMC_CUDA(tamc::copy_async(e.data(), d_e.p, R * 4, cudaMemcpyDeviceToHost, st));
     TAMC_CUDA(cudaStreamSynchronize(st));
     for (uint32_t r = 0; r < R; ++r)
       for (uint32_t i = 0; i < n; ++i)

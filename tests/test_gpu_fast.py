@@ -172,15 +172,34 @@ def test_pt_fast_deterministic_and_resumable(tb, po, gpu):
     assert np.array_equal(np.array(a.samples().e), np.array(c.samples().e))
 
 
-def test_pt_fast_qubo_energies_follow_reference_cache_rule(tb, po, gpu):
+@pytest.mark.parametrize("mode,form", [("fast", "fused"), ("fast", "plain"), ("ref", "fused")])
+@pytest.mark.parametrize("threads", [1, 3])
+def test_pt_qubo_energies_follow_reference_cache_rule(tb, po, gpu, monkeypatch, mode, form, threads):
     """With the QUBO diagonal stored as a self-coupling, the reference's cached
-    energy drifts from energy_ref between ICM refreshes; the fast mode keeps
-    both and reports the cache exactly as the reference would (up to f32)."""
-    text = gi.qubo_er(64, 5, 2)
-    b = po.geometric_betas(0.1, 1.0, 8)
-    run = tb.PtRun(gpu.upload(tb.HostInstance.parse(text, qubo=True)), _pt(tb, 100, b, 4), 4).run().sync()
+    energy drifts from energy_ref by -2 K_ii per accepted flip and is reset at
+    every Houdayer invalidation.  With an all-zero ladder the drift of every
+    measured energy is predicted exactly (tests/qubo_rule.py); the reported
+    e samples of every round, slot and chain must equal the FP64 energy of the
+    sampled state plus that drift, within 1e-5 relative.  This is the energy the
+    serving path reports on QUBO requests."""
+    from qubo_rule import check_cached_energies, self_coupling_sum, sweeps_since_refresh
+    text = gi.qubo_er(48, 5, 2)
+    h = tb.HostInstance.parse(text, qubo=True)
+    rp, col, K, _ = h.csr()
+    ksum = self_coupling_sum(rp, col, K)
+    assert ksum != 0.0
+    nt, lo, rounds, C = 6, 3, 14, 2
+    monkeypatch.setenv("TAMC_PT_FORM", form)  # colour-ordered mode's two forms; ignored in reference order
+    p = tb.PtParams(rounds, np.zeros(nt, np.float32), lo, 0.0, True, C, threads, 1, 1, 0)
+    run = tb.PtRun(gpu.upload(h), p, 5, tb.MODE_FAST if mode == "fast" else tb.MODE_REF).run().sync()
+    ts = run.samples()
+    inst = po.Instance.from_text(text, qubo=True)
+    assert check_cached_energies(ts.e, ts.samples, inst.energy_f64, nt, lo, rounds, C, ksum, h.n) >= 3
+    # the final cached energies follow the same rule
     S, E = run.state()
-    assert np.all(np.isfinite(E))
+    m_last = sweeps_since_refresh(nt, lo, rounds)[-1]
+    want = np.array([[inst.energy_f64(S[c, t]) - 2.0 * m_last[t] * ksum for t in range(nt)] for c in range(C)])
+    assert np.all(np.abs(E - want) <= 1e-5 * np.maximum(np.abs(want), 1.0))
 
 
 # -------------------------------------------------- batched and serving ----
@@ -253,6 +272,50 @@ def test_server_admission_and_target_energy(tb, gpu):
     with pytest.raises(tb.TamcError) as e:
         tiny.submit(h, p, 1)
     assert e.value.code == -9
+
+
+def test_server_cancel_and_failed_admission(tb, po, gpu):
+    """Host-side failure paths of the serving loop: a queued request cancelled
+    never runs; an active one cancelled between steps keeps the replicas it
+    had (energies still match FP64) and frees its slot at once; a request the
+    device refuses at admission (an instance without sites) fails alone with
+    its reason; the request that runs beside them gives the same result as
+    alone, bit for bit."""
+    jobs = _mixed_jobs(po, 3, 2)
+    srv = tb.Server(gpu, hbm_budget_bytes=1 << 30, max_active=1, chunk_sweeps=20)
+    hs = [tb.HostInstance.parse(t) for t, _, _ in jobs]
+    ps = [tb.PtParams(200, b, lo, 0.5, True, 2, 4) for _, b, lo in jobs]
+    a = srv.submit(hs[0], ps[0], 11)
+    empty = tb.HostInstance.from_csr(np.zeros(1, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.float32),
+                                     np.zeros(0, np.float32))
+    bad = srv.submit(empty, ps[0], 99)
+    c = srv.submit(hs[1], ps[1], 12)
+    d = srv.submit(hs[2], ps[2], 13)
+    srv.cancel(d)
+    assert srv.status(d) == ("cancelled", "")
+    assert srv.result(d)[0] and srv.result(d)[2] == 0
+    assert srv.step() == (1, 2)
+    assert srv.status(a)[0] == "active"
+    srv.cancel(a)
+    assert srv.status(a)[0] == "cancelled"
+    done, best, sweeps, lat = srv.result(a)
+    assert done and 0 < sweeps < 200 and lat > 0
+    S, E = srv.state(a)
+    want = _f64_energies(po, jobs[0][0], S)
+    assert _rel_ok(E, want)
+    for bad_call in (lambda: srv.cancel(a), lambda: srv.state(d)):
+        with pytest.raises(tb.TamcError) as e:
+            bad_call()
+        assert e.value.code == -1
+    while srv.step() != (0, 0):
+        pass
+    st, why = srv.status(bad)
+    assert st == "failed" and "no sites" in why and srv.result(bad)[0]
+    assert srv.status(c)[0] == "done"
+    alone = tb.PtRun(gpu.upload(hs[1]), ps[1], 12).run().sync()
+    S1, E1 = alone.state()
+    S2, E2 = srv.state(c)
+    assert np.array_equal(S1, S2) and np.array_equal(E1, E2)
 
 
 def test_server_largest_request_size(tb, gpu):

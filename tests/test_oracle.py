@@ -192,3 +192,63 @@ def test_threaded_run_independent_of_omp_threads(po):
         r.run(nthreads=nth)
         outs.append(r.states()[0])
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("threads", [1, 3])
+def test_oracle_qubo_cached_energy_rule(po, threads):
+    """The oracle's cached energies on a QUBO follow the reference's rule
+    (self-coupling drift between Houdayer refreshes), predicted exactly with an
+    all-zero ladder; pins the predictor the GPU test uses."""
+    from qubo_rule import check_cached_energies, self_coupling_sum
+    from tamc_b200 import instances as gi
+    inst = po.Instance.from_text(gi.qubo_er(48, 5, 2), qubo=True)
+    rp, col, K, _ = inst.csr()
+    ksum = self_coupling_sum(rp, col, K)
+    assert ksum != 0.0
+    nt, lo, rounds, C = 6, 3, 14, 2
+    orc = po.PtRun(inst, np.zeros(nt, np.float32), rounds, 0.0, lo, True, C, threads, sample=1, sample_states=1,
+                   sample_limiting=0, seed=5)
+    orc.run()
+    e, _, _, samples = orc.thermal()
+    assert check_cached_energies(e, samples, inst.energy_f64, nt, lo, rounds, C, ksum, inst.n) >= 3
+
+
+@pytest.mark.parametrize("case", range(8))
+def test_pt_opt_step_matches_restatement(tb, case):
+    """tamc_pt_opt_step (the library's ladder update) against the oracle's
+    float32 restatement of pt_optimize_beta's iteration, bit for bit, on
+    synthetic round-trip statistics (including zero round trips and too few
+    to form the density)."""
+    import ctypes as C
+    import ptopt
+    rng = np.random.default_rng(case)
+    nt = [8, 12, 16, 32, 24, 9, 16, 5][case]
+    ninst = [1, 3, 5, 2, 4, 1, 6, 2][case]
+    betas = tb.geometric_betas(0.2, 5.0, nt)
+    mom = betas * np.float32(1.03) if case % 2 else betas.copy()
+    rts = rng.integers(0, 40, ninst).astype(np.uint32)
+    if case == 5:
+        rts[:] = 0
+    frac = 1 / (1 + np.exp(-np.linspace(-4, 4, nt) + rng.normal(0, 0.3, nt)))
+    tot = rng.integers(500, 5000, (ninst, nt))
+    dh = np.stack([tot - np.round(tot * frac), np.round(tot * frac)], -1).astype(np.uint32)
+    if case == 7:
+        dh[:] = 0  # no flow at all: every fraction 1/2, no density
+    want = ptopt.step(betas, mom, rts, dh, 2000, 2, 0.2, 0.85)
+    b, m = betas.copy(), mom.copy().astype(np.float32)
+    tau = np.zeros(ninst, np.float32)
+    err = C.c_float()
+    L = tb.lib()
+    L.tamc_pt_opt_step.restype = C.c_int
+    rc = L.tamc_pt_opt_step(nt, b.ctypes.data_as(C.POINTER(C.c_float)), m.ctypes.data_as(C.POINTER(C.c_float)),
+                            ninst, np.ascontiguousarray(rts).ctypes.data_as(C.POINTER(C.c_uint32)),
+                            np.ascontiguousarray(dh).ctypes.data_as(C.POINTER(C.c_uint32)), 2000, 2,
+                            C.c_float(0.2), C.c_float(0.85), tau.ctypes.data_as(C.POINTER(C.c_float)),
+                            C.byref(err))
+    assert rc == want[0]
+    assert np.array_equal(tau.view(np.uint32), np.array(want[3], np.float32).view(np.uint32))
+    assert np.array_equal(b.view(np.uint32), np.array(want[1], np.float32).view(np.uint32))
+    assert np.array_equal(m.view(np.uint32), np.array(want[2], np.float32).view(np.uint32))
+    if rc == 0:
+        assert np.float32(err.value) == want[4]
+        assert np.all(np.diff(b) > 0) and b[0] == betas[0]
