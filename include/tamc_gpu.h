@@ -118,6 +118,10 @@ int tamc_method_pt(const tamc_method* m, tamc_pt_params* p);
 /* SA (SaParams, src/sa.rs:21-26): beta array (points into m), replicas, threads. */
 int tamc_method_sa(const tamc_method* m, const float** betas, uint32_t* nbeta, uint32_t* num_replicas,
                    uint32_t* threads);
+/* GLA (GlaParams, src/gla.rs:28-33): num_threads, the partition file path
+ * (points into m), and the sub-solver's PtIcmParams (`pt_params`) as
+ * tamc_method_pt reports them; any output pointer may be NULL. */
+int tamc_method_gla(const tamc_method* m, uint32_t* num_threads, const char** partition_file, tamc_pt_params* p);
 void tamc_method_free(tamc_method* m);
 /* geometric_beta_schedule (tamc-core/src/sa.rs:13-22) cast to f32. */
 int tamc_geometric_betas(float beta_min, float beta_max, uint32_t n, float* out);
@@ -135,6 +139,9 @@ int tamc_gpu_sync(tamc_gpu* g);
 void* tamc_gpu_stream(tamc_gpu* g);
 /* Number of kernels this context launched so far (for accounting). */
 uint64_t tamc_gpu_launch_count(tamc_gpu* g);
+/* Bytes the library has copied host->device and device->host since it was
+ * loaded, over all contexts (for end-to-end accounting). */
+void tamc_copy_bytes(uint64_t* h2d, uint64_t* d2h);
 
 /* Uploads the instance: reference-order CSR, ICM graph, colour-sorted CSR for
  * the fast mode and the susceptibility weights.  An instance with no sites is
@@ -250,16 +257,83 @@ int tamc_gpu_batch_sync(tamc_batch* b);
 /* Per-job results, same layouts as the tamc_gpu_pt_* getters. */
 int tamc_gpu_batch_get_state(tamc_batch* b, uint32_t job, int8_t* spins, float* energies);
 int tamc_gpu_batch_acceptance(tamc_batch* b, uint32_t job, uint32_t* counts);
+/* Replaces a job's replicas before its run (PtIcmRunner::run(Some(states)), src/pt.rs:397-407). */
+int tamc_gpu_batch_set_state(tamc_batch* b, uint32_t job, const int8_t* spins);
+int tamc_gpu_batch_round_trips(tamc_batch* b, uint32_t job, uint8_t* tags, uint32_t* round_trips,
+                               uint32_t* diffusion_hist);
 int tamc_gpu_batch_gs(tamc_batch* b, uint32_t job, uint32_t cap, uint32_t* count, uint32_t* steps,
                       float* energies, uint64_t* states);
 int tamc_gpu_batch_samples_dims(tamc_batch* b, uint32_t job, uint32_t* M, uint32_t* S, uint32_t* Z,
                                 uint32_t* nchi);
 int tamc_gpu_batch_samples(tamc_batch* b, uint32_t job, float* e, int32_t* q, float* suscept,
                            uint8_t* samples);
+/* Device time of the batch's kernel launches so far: the sum of CUDA-event
+ * times around each chunk launch (job-table upload, the persistent kernel,
+ * count readback), and the number of such launches. */
+int tamc_gpu_batch_device_time(tamc_batch* b, double* ms, uint64_t* launches);
 /* Autotuner choice for a job: threads per CTA, slots per task, smem residency. */
 int tamc_gpu_batch_tile(tamc_batch* b, uint32_t job, uint32_t* cta_threads, uint32_t* slots_per_task,
                         int32_t* csr_in_smem);
 int tamc_gpu_batch_destroy(tamc_batch* b);
+
+/* ------------------------------------------------------------------------
+ * GLA partitioned solve.  Replaces run_gla (src/gla.rs:121-195): the instance
+ * is split into the sub-instances induced by a partition of its sites
+ * (induced_subgraph_instance_sorted, src/ising.rs:327-355), each is solved by
+ * PT-ICM with PtIcmRunner::pt_loop semantics (single stream, serial
+ * exchange, whatever pt_params.threads says), and the last ground state of
+ * every sub-run is joined with the couplings that cross partitions.
+ * TAMC_MODE_FAST runs all sub-instances as one batch; TAMC_MODE_REF runs one
+ * reference-order replay per sub-instance on the Xoshiro256++ stream
+ * seed_from_u64(seed) cloned and jumped once per sub-instance (the
+ * reference draws that master stream's seed from OS entropy). */
+typedef struct tamc_partition tamc_partition;
+typedef struct tamc_gla tamc_gla;
+
+/* GlaParams::read_graph_partition (src/gla.rs:37-58) over read_u32_lines
+ * (src/util.rs:142-172): one partition per line of whitespace-separated site
+ * indices (lines without a leading index are skipped, text after the last
+ * index is ignored); an index >= n or listed twice is TAMC_E_INVAL. */
+int tamc_partition_parse(const char* text, uint64_t len, uint32_t n, tamc_partition** out);
+int tamc_partition_read(const char* path, uint32_t n, tamc_partition** out);
+int tamc_partition_dims(const tamc_partition* p, uint32_t* num_parts, uint64_t* num_sites);
+/* part_ptr[num_parts + 1] offsets into sites[num_sites], partitions in file order. */
+int tamc_partition_get(const tamc_partition* p, uint32_t* part_ptr, uint32_t* sites);
+void tamc_partition_free(tamc_partition* p);
+
+/* Runs the solve.  Inputs on which the reference panics (a site in no
+ * partition, a last site without couplings, a sub-run without a recorded
+ * ground state) return TAMC_E_REFPANIC. */
+int tamc_gla_run(tamc_gpu* g, const tamc_host_instance* inst, const tamc_partition* part, const tamc_pt_params* p,
+                 uint64_t seed, int mode, tamc_gla** out);
+/* GlaResults (src/gla.rs:61-69) sizes and fields: partition_energies[num_partitions],
+ * boundary_energies as (bnd_src, bnd_dst, bnd_energies)[num_boundaries], total_energy. */
+int tamc_gla_dims(const tamc_gla* r, uint32_t* instance_size, uint32_t* num_partitions, uint32_t* num_boundaries);
+int tamc_gla_results(const tamc_gla* r, float* partition_energies, uint32_t* bnd_src, uint32_t* bnd_dst,
+                     float* bnd_energies, float* total_energy);
+/* The partitions' ground states joined into one state of the whole instance
+ * (int8 +-1, n entries).  The reference leaves GlaResults.final_state empty. */
+int tamc_gla_state(const tamc_gla* r, int8_t* spins);
+/* write_data (src/util.rs:26-36): pickle for a `.pkl` path, else bincode. */
+int tamc_gla_write(const tamc_gla* r, const char* path);
+void tamc_gla_free(tamc_gla* r);
+
+/* ------------------------------------------------------------------------
+ * Temperature-ladder optimisation (tamc-pt-opt).  One update of
+ * pt_optimize_beta (src/bin/tamc-pt-opt.rs:59-181) from the statistics that
+ * PT runs at the current ladder recorded: round_trips[num_instances] and
+ * diffusion_hist[num_instances][nt][2], each summed over the instance's
+ * chains (tamc_gpu_pt_round_trips / tamc_gpu_batch_round_trips).  betas[nt]
+ * is replaced by the next ladder and momentum[nt] (the first ladder on the
+ * first call) updated; tau[num_instances] receives the round-trip times in
+ * sweeps and *err the mean |log10| change of the interior betas.  f32
+ * arithmetic in the reference's order.  Returns TAMC_OK; 1 when the runs saw
+ * too few round trips ("Insufficient round trips for eta CDF": betas and
+ * momentum unchanged, tau still written); TAMC_E_REFPANIC where the
+ * reference's bisection panics. */
+int tamc_pt_opt_step(uint32_t nt, float* betas, float* momentum, uint32_t num_instances,
+                     const uint32_t* round_trips, const uint32_t* diffusion_hist, uint32_t num_sweeps,
+                     uint32_t num_chains, float alpha, float m, float* tau, float* err);
 
 /* ------------------------------------------------------------------------
  * Serving: continuous batching of solve requests.  Requests arriving while
@@ -277,12 +351,28 @@ int tamc_serve_submit(tamc_server* s, const tamc_host_instance* inst, const tamc
 /* One scheduling step: admit, run one chunk of rounds for all active requests,
  * retire finished ones.  *active / *queued report the counts afterwards. */
 int tamc_serve_step(tamc_server* s, uint32_t* active, uint32_t* queued);
-/* Result of a retired request: done flag, best energy, sweeps run, latency
- * from submit to retirement in seconds. */
+/* Result of a request: done flag (it has ended: finished, cancelled or
+ * failed), best energy so far, sweeps run, latency from submit to its end
+ * in seconds (-1 while it has not ended). */
 int tamc_serve_result(tamc_server* s, uint64_t request_id, int32_t* done, float* best_energy,
                       uint32_t* sweeps, double* latency_s);
-/* Final slot-ordered state of a retired request (as tamc_gpu_pt_get_state). */
+/* Final slot-ordered state of a request that ran and ended (finished, or
+ * cancelled while active), as tamc_gpu_pt_get_state. */
 int tamc_serve_state(tamc_server* s, uint64_t request_id, int8_t* spins, float* energies);
+/* Request states reported by tamc_serve_status. */
+#define TAMC_REQ_QUEUED 0
+#define TAMC_REQ_ACTIVE 1
+#define TAMC_REQ_DONE 2      /* sweep budget or target energy reached */
+#define TAMC_REQ_CANCELLED 3 /* tamc_serve_cancel */
+#define TAMC_REQ_FAILED 4    /* refused at admission; *error says why */
+/* State of a request, and for a failed one the reason (valid until the
+ * server is destroyed). */
+int tamc_serve_status(tamc_server* s, uint64_t request_id, int32_t* status, const char** error);
+/* Cancels a queued request (it never runs) or an active one (stopped between
+ * steps: its replicas so far are kept as its final state, its device memory
+ * and HBM budget are released at once).  Other requests are unaffected.
+ * TAMC_E_INVAL for a request that has already ended. */
+int tamc_serve_cancel(tamc_server* s, uint64_t request_id);
 int tamc_serve_destroy(tamc_server* s);
 
 #ifdef __cplusplus

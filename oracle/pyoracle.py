@@ -83,6 +83,10 @@ def lib():
             "orc_pt_icm_sizes": (None, [C.c_void_p, i64p]),
             "orc_sa_run": (C.c_uint32, [C.c_void_p, f32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                         C.c_int, f32p, i8p]),
+            "orc_gla_run": (C.c_int, [C.c_void_p, u32p, u32p, C.c_uint32, C.c_uint32, C.c_double, f32p,
+                                      C.c_uint32, C.c_uint32, C.c_int, C.c_uint32, C.c_int64, C.c_int64,
+                                      C.c_uint32, C.c_uint64, f32p, C.c_uint32, u32p, u32p, u32p, f32p, f32p,
+                                      i8p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -325,3 +329,34 @@ def sa_run(inst: Instance, betas, num_replicas, threads, seed, nthreads=0):
     if got != r:
         raise ValueError("bad SA parameters")
     return e, s
+
+
+def gla_run(inst: Instance, parts, betas, num_sweeps, warmup_fraction=0.5, lo_beta_idx=0, icm=True,
+            num_chains=2, sample=None, sample_states=None, sample_limiting=0, seed=0):
+    """run_gla (src/gla.rs:121-195) with the master stream seed_from_u64(seed):
+    dict of GlaResults fields plus the joined state; None where the reference panics."""
+    b = np.ascontiguousarray(betas, np.float32)
+    ptr = np.zeros(len(parts) + 1, np.uint32)
+    ptr[1:] = np.cumsum([len(p) for p in parts])
+    sites = np.ascontiguousarray(np.concatenate([np.asarray(p, np.uint32) for p in parts]) if parts else
+                                 np.zeros(0, np.uint32), np.uint32)
+    cap = max(1, len(parts) * len(parts))
+    pe = np.zeros(len(parts), np.float32)
+    nb = C.c_uint32()
+    bs, bd = np.zeros(cap, np.uint32), np.zeros(cap, np.uint32)
+    be = np.zeros(cap, np.float32)
+    tot = C.c_float()
+    joined = np.zeros(inst.n, np.int8)
+    rc = lib().orc_gla_run(inst.h, _p(ptr, u32p), _p(sites, u32p), len(parts), num_sweeps, warmup_fraction,
+                           _p(b, f32p), len(b), lo_beta_idx, int(icm), num_chains,
+                           -1 if sample is None else sample, -1 if sample_states is None else sample_states,
+                           sample_limiting, seed, _p(pe, f32p), cap, C.byref(nb), _p(bs, u32p), _p(bd, u32p),
+                           _p(be, f32p), C.byref(tot), _p(joined, i8p))
+    if rc == -2:
+        return None
+    if rc != 0:
+        raise ValueError("bad GLA input")
+    k = nb.value
+    return {"instance_size": inst.n, "num_partitions": len(parts), "partition_energies": pe,
+            "boundary_energies": list(zip(bs[:k].tolist(), bd[:k].tolist(), be[:k].tolist())),
+            "bnd_energies": be[:k], "total_energy": np.float32(tot.value), "state": joined}

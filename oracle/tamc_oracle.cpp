@@ -120,12 +120,15 @@ struct Instance {
   std::vector<std::vector<double>> suscept;  // src/ising.rs:388-403
 };
 
-static void build_icm_graph(Instance& I) {
+// diag: the sprs `coupling` matrix also holds the diagonal entries, as in the
+// sub-instances GLA builds (src/ising.rs:327-355: every kept row entry goes
+// into the triplet matrix); self-loops only extend the node range.
+static void build_icm_graph(Instance& I, bool diag = false) {
   uint32_t maxn = 0;
   bool any = false;
   for (uint32_t i = 0; i < I.n; ++i)
     for (uint32_t e = I.row_ptr[i]; e < I.row_ptr[i + 1]; ++e)
-      if (I.col[e] != i) { any = true; maxn = std::max(maxn, std::max(i, I.col[e])); }
+      if (I.col[e] != i || diag) { any = true; maxn = std::max(maxn, std::max(i, I.col[e])); }
   I.g_nodes = any ? maxn + 1 : 0;
   I.g_row_ptr.assign(I.g_nodes + 1, 0);
   I.g_col.clear();
@@ -648,9 +651,9 @@ float orc_delta_energy(const void* h, const int8_t* s, uint32_t i) { return delt
 
 // -- PT-ICM runner (PtIcmRunner::run / run_parallel, src/pt.rs:354-412).
 // sample/sample_states < 0 mean None.
-void* orc_pt_new(const void* inst, uint32_t num_sweeps, double warmup_fraction, const float* betas,
-                 uint32_t nb, uint32_t lo_beta_idx, int icm, uint32_t num_chains, uint32_t threads,
-                 int64_t sample, int64_t sample_states, uint32_t sample_limiting, uint64_t seed) {
+static PtRun* pt_make(const void* inst, uint32_t num_sweeps, double warmup_fraction, const float* betas,
+                      uint32_t nb, uint32_t lo_beta_idx, int icm, uint32_t num_chains, uint32_t threads,
+                      int64_t sample, int64_t sample_states, uint32_t sample_limiting, Xoshiro master) {
   PtRun* R = new PtRun();
   R->I = (const Instance*)inst;
   R->P.num_sweeps = num_sweeps;
@@ -667,7 +670,7 @@ void* orc_pt_new(const void* inst, uint32_t num_sweeps, double warmup_fraction, 
   for (uint32_t k = 0; k + 1 < nb; ++k) R->delta_beta.push_back(betas[k + 1] - betas[k]);
   const double mi = warmup_fraction * (double)num_sweeps;
   R->meas_init = mi <= 0.0 ? 0u : (mi >= 4294967295.0 ? 0xffffffffu : (uint32_t)mi);
-  R->rng = seed_from_u64(seed);
+  R->rng = master;
   for (uint32_t c = 0; c < num_chains; ++c) {  // generate_init_state (src/pt.rs:506-519)
     std::vector<IsingState> st;
     for (uint32_t t = 0; t < nb; ++t) st.push_back(rand_state(*R->I, R->rng));
@@ -685,6 +688,12 @@ void* orc_pt_new(const void* inst, uint32_t num_sweeps, double warmup_fraction, 
   else if (R->P.sample_limiting == 1) R->samples.resize(nb / 2);
   else R->samples.resize(1);
   return R;
+}
+void* orc_pt_new(const void* inst, uint32_t num_sweeps, double warmup_fraction, const float* betas,
+                 uint32_t nb, uint32_t lo_beta_idx, int icm, uint32_t num_chains, uint32_t threads,
+                 int64_t sample, int64_t sample_states, uint32_t sample_limiting, uint64_t seed) {
+  return pt_make(inst, num_sweeps, warmup_fraction, betas, nb, lo_beta_idx, icm, num_chains, threads, sample,
+                 sample_states, sample_limiting, seed_from_u64(seed));
 }
 void orc_pt_free(void* h) { delete (PtRun*)h; }
 const char* orc_pt_error(void* h) { return ((PtRun*)h)->err.c_str(); }
@@ -814,3 +823,107 @@ uint32_t orc_sa_run(const void* inst, const float* betas, uint32_t nbeta, uint32
 // Bounded SA sample for timing: runs `parts` partitions of `per` replicas for
 // nbeta sweeps; same code path as orc_sa_run.
 }  // extern "C"
+
+// -- GLA (run_gla, src/gla.rs:121-195) with the master stream seed_from_u64(seed)
+// in place of the reference's OS-entropy seed.  Partition k is
+// sites[part_ptr[k] .. part_ptr[k+1]) (file order, already checked as
+// read_graph_partition does).  Writes part_e[nparts], up to bnd_cap boundary
+// groups (count in *nbnd), *total and the joined state joined[n].
+// Returns 0, -2 where the reference panics, -3 if bnd_cap is too small.
+extern "C" int orc_gla_run(const void* inst, const uint32_t* part_ptr, const uint32_t* sites, uint32_t nparts,
+                           uint32_t num_sweeps, double warmup_fraction, const float* betas, uint32_t nb,
+                           uint32_t lo_beta_idx, int icm, uint32_t num_chains, int64_t sample,
+                           int64_t sample_states, uint32_t sample_limiting, uint64_t seed, float* part_e,
+                           uint32_t bnd_cap, uint32_t* nbnd, uint32_t* bnd_src, uint32_t* bnd_dst, float* bnd_e,
+                           float* total, int8_t* joined) {
+  const Instance& I = *(const Instance*)inst;
+  // to_energy_graph (src/ising.rs:414-425): coupling entries with i < j
+  struct E { uint32_t i, j; float K; };
+  std::vector<E> edges;
+  uint32_t nodes = 0;
+  for (uint32_t i = 0; i < I.n; ++i)
+    for (uint32_t e = I.row_ptr[i]; e < I.row_ptr[i + 1]; ++e)
+      if (I.col[e] > i) { edges.push_back(E{i, I.col[e], I.K[e]}); nodes = std::max(nodes, I.col[e] + 1); }
+  if (nodes < I.n) return -2;  // g[NodeIndex::new(i)] = h past the graph's nodes
+  std::vector<int64_t> pmap(I.n, -1);
+  std::vector<std::vector<uint32_t>> parts(nparts);
+  for (uint32_t k = 0; k < nparts; ++k) {
+    parts[k].assign(sites + part_ptr[k], sites + part_ptr[k + 1]);
+    for (uint32_t x : parts[k]) pmap[x] = k;
+    std::sort(parts[k].begin(), parts[k].end());  // partition_graph.add_node(p sorted)
+  }
+  for (uint32_t i = 0; i < nodes; ++i)
+    if (pmap[i] < 0) return -2;  // partition_mapping[&i] on a missing key
+  // partition graph: directed edge (p_i, p_j) per first appearance
+  std::vector<std::pair<uint32_t, uint32_t>> keys;
+  std::vector<std::vector<E>> groups;
+  for (const E& e : edges) {
+    const uint32_t a = (uint32_t)pmap[e.i], b = (uint32_t)pmap[e.j];
+    if (a == b) continue;
+    size_t x = 0;
+    while (x < keys.size() && !(keys[x].first == a && keys[x].second == b)) ++x;
+    if (x == keys.size()) { keys.emplace_back(a, b); groups.emplace_back(); }
+    groups[x].push_back(e);
+  }
+  if (keys.size() > bnd_cap) return -3;
+  // sub-instances (induced_subgraph_instance_sorted) and their runs:
+  // rng_vec[k] = master cloned, then jumped; init and pt_loop on it
+  Xoshiro master = seed_from_u64(seed);
+  std::vector<std::vector<int8_t>> best(nparts);
+  for (uint32_t k = 0; k < nparts; ++k) {
+    const std::vector<uint32_t>& nodes_k = parts[k];
+    Instance S;
+    S.n = (uint32_t)nodes_k.size();
+    S.offset = 0.0f;
+    S.row_ptr.push_back(0);
+    for (uint32_t ni : nodes_k) {
+      S.bias.push_back(I.bias[ni]);
+      for (uint32_t e = I.row_ptr[ni]; e < I.row_ptr[ni + 1]; ++e) {
+        auto it = std::lower_bound(nodes_k.begin(), nodes_k.end(), I.col[e]);
+        if (it != nodes_k.end() && *it == I.col[e]) {
+          S.col.push_back((uint32_t)(it - nodes_k.begin()));
+          S.K.push_back(I.K[e]);
+        }
+      }
+      S.row_ptr.push_back((uint32_t)S.col.size());
+    }
+    for (const auto& w : I.suscept) {
+      std::vector<double> sw;
+      for (uint32_t ni : nodes_k) sw.push_back(w[ni]);
+      S.suscept.push_back(sw);
+    }
+    build_icm_graph(S, true);
+    Xoshiro rk = master;
+    master.jump();
+    PtRun* R = pt_make(&S, num_sweeps, warmup_fraction, betas, nb, lo_beta_idx, icm, num_chains, 1, sample,
+                       sample_states, sample_limiting, rk);
+    const int rc = orc_pt_run(R, num_sweeps, 0);  // serial loop: no OpenMP
+    if (rc != 0 || R->gs.empty()) { delete R; return -2; }
+    part_e[k] = R->gs.back().energy;
+    best[k].assign(S.n, 1);
+    for (uint32_t i = 0; i < S.n; ++i) best[k][i] = ((R->gs.back().state[i / 64] >> (i % 64)) & 1u) ? -1 : 1;
+    delete R;
+  }
+  float bulk = 0.0f;
+  for (uint32_t k = 0; k < nparts; ++k) bulk += part_e[k];
+  float tb = 0.0f;
+  for (size_t x = 0; x < keys.size(); ++x) {
+    const uint32_t a = keys[x].first, b = keys[x].second;
+    float bnd = 0.0f;
+    for (const E& e : groups[x]) {
+      const size_t is = std::lower_bound(parts[a].begin(), parts[a].end(), e.i) - parts[a].begin();
+      const size_t js = std::lower_bound(parts[b].begin(), parts[b].end(), e.j) - parts[b].begin();
+      const int8_t prod = (int8_t)(best[a][is] * best[b][js]);
+      bnd += e.K * (float)prod;
+    }
+    tb += bnd;
+    bnd_src[x] = a;
+    bnd_dst[x] = b;
+    bnd_e[x] = bnd;
+  }
+  *nbnd = (uint32_t)keys.size();
+  *total = bulk + tb;
+  for (uint32_t k = 0; k < nparts; ++k)
+    for (size_t x = 0; x < parts[k].size(); ++x) joined[parts[k][x]] = best[k][x];
+  return 0;
+}

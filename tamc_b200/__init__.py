@@ -21,6 +21,7 @@ import numpy as np
 __all__ = [
     "TamcError", "lib", "HostInstance", "Method", "PtParams", "Gpu", "DeviceInstance", "PtRun", "sa_run",
     "sa_run_device", "Batch", "Server", "PtIcmRunner", "SaRunner", "geometric_betas", "MODE_REF", "MODE_FAST",
+    "Partition", "GlaResults", "gla_run", "pt_opt_step",
 ]
 
 MODE_REF = 0
@@ -28,6 +29,7 @@ MODE_FAST = 1
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtamc_b200.so")
 CLI_PATH = os.path.join(_HERE, "bin", "tamc_b200")
+PT_OPT_CLI_PATH = os.path.join(_HERE, "bin", "tamc_b200_pt_opt")
 
 ERRORS = {-1: "INVAL", -2: "NOMEM", -3: "CUDA", -4: "TIMEOUT", -5: "PARSE", -6: "IO", -7: "UNSUPPORTED",
           -8: "REFPANIC", -9: "ADMISSION"}
@@ -79,12 +81,25 @@ _SIGS = {
     "tamc_method_pt": (C.c_int, [vp, C.POINTER(_PtParams)]),
     "tamc_method_sa": (C.c_int, [vp, C.POINTER(f32p), u32p, u32p, u32p]),
     "tamc_method_free": (None, [vp]),
+    "tamc_method_gla": (C.c_int, [vp, u32p, C.POINTER(C.c_char_p), C.POINTER(_PtParams)]),
+    "tamc_partition_parse": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint32, C.POINTER(vp)]),
+    "tamc_partition_read": (C.c_int, [C.c_char_p, C.c_uint32, C.POINTER(vp)]),
+    "tamc_partition_dims": (C.c_int, [vp, u32p, u64p]),
+    "tamc_partition_get": (C.c_int, [vp, u32p, u32p]),
+    "tamc_partition_free": (None, [vp]),
+    "tamc_gla_run": (C.c_int, [vp, vp, vp, C.POINTER(_PtParams), C.c_uint64, C.c_int, C.POINTER(vp)]),
+    "tamc_gla_dims": (C.c_int, [vp, u32p, u32p, u32p]),
+    "tamc_gla_results": (C.c_int, [vp, f32p, u32p, u32p, f32p, f32p]),
+    "tamc_gla_state": (C.c_int, [vp, i8p]),
+    "tamc_gla_write": (C.c_int, [vp, C.c_char_p]),
+    "tamc_gla_free": (None, [vp]),
     "tamc_geometric_betas": (C.c_int, [C.c_float, C.c_float, C.c_uint32, f32p]),
     "tamc_gpu_open": (C.c_int, [C.c_int, C.POINTER(vp)]),
     "tamc_gpu_close": (C.c_int, [vp]),
     "tamc_gpu_sync": (C.c_int, [vp]),
     "tamc_gpu_stream": (vp, [vp]),
     "tamc_gpu_launch_count": (C.c_uint64, [vp]),
+    "tamc_copy_bytes": (None, [u64p, u64p]),
     "tamc_gpu_instance_upload": (C.c_int, [vp, vp, C.POINTER(vp)]),
     "tamc_gpu_instance_destroy": (C.c_int, [vp]),
     "tamc_gpu_pt_create": (C.c_int, [vp, C.POINTER(_PtParams), C.c_uint64, C.c_int, C.POINTER(vp)]),
@@ -114,6 +129,11 @@ _SIGS = {
     "tamc_gpu_batch_gs": (C.c_int, [vp, C.c_uint32, C.c_uint32, u32p, u32p, f32p, u64p]),
     "tamc_gpu_batch_samples_dims": (C.c_int, [vp, C.c_uint32, u32p, u32p, u32p, u32p]),
     "tamc_gpu_batch_samples": (C.c_int, [vp, C.c_uint32, f32p, i32p, f32p, u8p]),
+    "tamc_gpu_batch_device_time": (C.c_int, [vp, f64p, u64p]),
+    "tamc_gpu_batch_set_state": (C.c_int, [vp, C.c_uint32, i8p]),
+    "tamc_gpu_batch_round_trips": (C.c_int, [vp, C.c_uint32, u8p, u32p, u32p]),
+    "tamc_pt_opt_step": (C.c_int, [C.c_uint32, f32p, f32p, C.c_uint32, u32p, u32p, C.c_uint32, C.c_uint32,
+                                   C.c_float, C.c_float, f32p, f32p]),
     "tamc_gpu_batch_tile": (C.c_int, [vp, C.c_uint32, u32p, u32p, i32p]),
     "tamc_gpu_batch_destroy": (C.c_int, [vp]),
     "tamc_serve_create": (C.c_int, [vp, C.c_uint64, C.c_uint32, C.c_uint32, C.POINTER(vp)]),
@@ -121,6 +141,8 @@ _SIGS = {
     "tamc_serve_step": (C.c_int, [vp, u32p, u32p]),
     "tamc_serve_result": (C.c_int, [vp, C.c_uint64, i32p, f32p, u32p, f64p]),
     "tamc_serve_state": (C.c_int, [vp, C.c_uint64, i8p, f32p]),
+    "tamc_serve_status": (C.c_int, [vp, C.c_uint64, i32p, C.POINTER(C.c_char_p)]),
+    "tamc_serve_cancel": (C.c_int, [vp, C.c_uint64]),
     "tamc_serve_destroy": (C.c_int, [vp]),
 }
 
@@ -153,6 +175,13 @@ def _check(rc: int) -> None:
 
 def _p(a: np.ndarray, t):
     return a.ctypes.data_as(t)
+
+
+def copy_bytes():
+    """(host->device, device->host) bytes the library has copied since load."""
+    h, d = C.c_uint64(), C.c_uint64()
+    lib().tamc_copy_bytes(C.byref(h), C.byref(d))
+    return h.value, d.value
 
 
 def geometric_betas(beta_min: float, beta_max: float, n: int) -> np.ndarray:
@@ -291,6 +320,18 @@ class Method:
         return PtParams(p.num_sweeps, betas, p.lo_beta_idx, p.warmup_fraction, bool(p.icm), p.num_replica_chains,
                         p.threads, None if p.sample < 0 else p.sample,
                         None if p.sample_states < 0 else p.sample_states, p.sample_limiting)
+
+    def gla(self):
+        """GLA: (num_threads, partition_file, the sub-solvers' PtParams)."""
+        nt = C.c_uint32()
+        pf = C.c_char_p()
+        p = _PtParams()
+        _check(lib().tamc_method_gla(self.h, C.byref(nt), C.byref(pf), C.byref(p)))
+        betas = np.ctypeslib.as_array(p.betas, shape=(p.num_beta,)).copy()
+        pt = PtParams(p.num_sweeps, betas, p.lo_beta_idx, p.warmup_fraction, bool(p.icm), p.num_replica_chains,
+                      p.threads, None if p.sample < 0 else p.sample,
+                      None if p.sample_states < 0 else p.sample_states, p.sample_limiting)
+        return nt.value, pf.value.decode(), pt
 
     def sa(self):
         b = f32p()
@@ -547,6 +588,41 @@ class Batch:
         _check(lib().tamc_gpu_batch_acceptance(self.h, job, _p(a, u32p)))
         return a
 
+    def set_state(self, job: int, spins) -> None:
+        a = np.ascontiguousarray(spins, np.int8)
+        _check(lib().tamc_gpu_batch_set_state(self.h, job, _p(a, i8p)))
+
+    def round_trips(self, job: int):
+        _, p = self.jobs[job]
+        nt, Cc = len(p.betas), p.num_replica_chains
+        t = np.zeros((Cc, nt), np.uint8)
+        r = np.zeros(Cc, np.uint32)
+        d = np.zeros((Cc, nt, 2), np.uint32)
+        _check(lib().tamc_gpu_batch_round_trips(self.h, job, _p(t, u8p), _p(r, u32p), _p(d, u32p)))
+        return t, r, d
+
+    def samples(self, job: int) -> "ThermalSamples":
+        """PtIcmThermalSamples of one job (as PtRun.samples)."""
+        d, p = self.jobs[job]
+        M, S, Z, nchi = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(lib().tamc_gpu_batch_samples_dims(self.h, job, C.byref(M), C.byref(S), C.byref(Z), C.byref(nchi)))
+        M, S, Z, nchi = M.value, S.value, Z.value, nchi.value
+        nt, Cc, nb = len(p.betas), p.num_replica_chains, (d.n + 7) // 8
+        P = Cc // 2
+        e = np.zeros((nt, M * Cc), np.float32)
+        q = np.zeros((nt, M * P), np.int32)
+        sus = np.zeros((nt, nchi, M * P), np.float32)
+        smp = np.zeros((Z, S * Cc, nb), np.uint8)
+        _check(lib().tamc_gpu_batch_samples(self.h, job, _p(e, f32p), _p(q, i32p), _p(sus, f32p), _p(smp, u8p)))
+        return ThermalSamples(p.sample_limiting, d.n, np.asarray(p.betas, np.float32), [list(z) for z in smp],
+                              list(e), list(q), [list(r) for r in sus])
+
+    def device_time(self):
+        """(summed CUDA-event ms of the chunk launches, number of launches)."""
+        ms, n = C.c_double(), C.c_uint64()
+        _check(lib().tamc_gpu_batch_device_time(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
     def tile(self, job: int):
         t, s, c = C.c_uint32(), C.c_uint32(), C.c_int32()
         _check(lib().tamc_gpu_batch_tile(self.h, job, C.byref(t), C.byref(s), C.byref(c)))
@@ -584,6 +660,18 @@ class Server:
         _check(lib().tamc_serve_result(self.h, rid, C.byref(d), C.byref(b), C.byref(s), C.byref(l)))
         return bool(d.value), b.value, s.value, l.value
 
+    STATUS = ("queued", "active", "done", "cancelled", "failed")
+
+    def status(self, rid: int):
+        """(state name, error message for a failed request or '')."""
+        st = C.c_int32()
+        err = C.c_char_p()
+        _check(lib().tamc_serve_status(self.h, rid, C.byref(st), C.byref(err)))
+        return self.STATUS[st.value], (err.value or b"").decode()
+
+    def cancel(self, rid: int) -> None:
+        _check(lib().tamc_serve_cancel(self.h, rid))
+
     def state(self, rid: int):
         n, p = self.params[rid]
         s = np.zeros((p.num_replica_chains, len(p.betas), n), np.int8)
@@ -595,6 +683,95 @@ class Server:
         if getattr(self, "h", None) and _lib is not None:
             _lib.tamc_serve_destroy(self.h)
             self.h = None
+
+
+# ------------------------------------------------------------- pt-opt
+def pt_opt_step(betas, momentum, round_trips, diffusion_hist, num_sweeps: int, num_chains: int, alpha: float,
+                m: float):
+    """One ladder update of tamc-pt-opt (tamc_pt_opt_step).  round_trips[I] and
+    diffusion_hist[I][nt][2] are per instance, summed over chains.  Returns
+    (updated, betas, momentum, tau, err); `updated` False when the runs saw too
+    few round trips (ladder and momentum unchanged, err None)."""
+    b = np.array(betas, np.float32)
+    mo = np.array(momentum, np.float32)
+    rt = np.ascontiguousarray(round_trips, np.uint32)
+    dh = np.ascontiguousarray(diffusion_hist, np.uint32)
+    tau = np.zeros(len(rt), np.float32)
+    err = C.c_float()
+    rc = lib().tamc_pt_opt_step(len(b), _p(b, f32p), _p(mo, f32p), len(rt), _p(rt, u32p), _p(dh, u32p), num_sweeps,
+                                num_chains, alpha, m, _p(tau, f32p), C.byref(err))
+    if rc == 1:
+        return False, b, mo, tau, None
+    _check(rc)
+    return True, b, mo, tau, err.value
+
+
+# ---------------------------------------------------------------- GLA
+class Partition:
+    """A site partition for GLA (GlaParams::read_graph_partition, src/gla.rs:37-58)."""
+
+    def __init__(self, handle):
+        self.h = handle
+        npart, nsite = C.c_uint32(), C.c_uint64()
+        _check(lib().tamc_partition_dims(self.h, C.byref(npart), C.byref(nsite)))
+        ptr = np.zeros(npart.value + 1, np.uint32)
+        sites = np.zeros(nsite.value, np.uint32)
+        _check(lib().tamc_partition_get(self.h, _p(ptr, u32p), _p(sites, u32p)))
+        self.parts = [sites[ptr[k]:ptr[k + 1]].tolist() for k in range(npart.value)]
+
+    @classmethod
+    def parse(cls, text: str | bytes, n: int) -> "Partition":
+        b = text.encode() if isinstance(text, str) else text
+        h = vp()
+        _check(lib().tamc_partition_parse(b, len(b), n, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def read(cls, path: str, n: int) -> "Partition":
+        h = vp()
+        _check(lib().tamc_partition_read(path.encode(), n, C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.tamc_partition_free(self.h)
+            self.h = None
+
+
+@dataclass
+class GlaResults:
+    """GlaResults (src/gla.rs:61-69), plus the joined ground state."""
+    instance_size: int
+    num_partitions: int
+    partition_energies: np.ndarray
+    boundary_energies: list
+    total_energy: float
+    state: np.ndarray
+
+
+def gla_run(gpu: Gpu, inst: HostInstance, part: Partition, params: PtParams, seed: int, mode: int = MODE_FAST,
+            output: Optional[str] = None) -> GlaResults:
+    """run_gla (src/gla.rs:121-195) on the device; `output` writes the result
+    file as the reference does (pickle for .pkl, else bincode)."""
+    cp = params.to_c()
+    h = vp()
+    _check(lib().tamc_gla_run(gpu.h, inst.h, part.h, C.byref(cp), seed, mode, C.byref(h)))
+    try:
+        n, npart, nb = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(lib().tamc_gla_dims(h, C.byref(n), C.byref(npart), C.byref(nb)))
+        pe = np.zeros(npart.value, np.float32)
+        bs, bd = np.zeros(nb.value, np.uint32), np.zeros(nb.value, np.uint32)
+        be = np.zeros(nb.value, np.float32)
+        tot = C.c_float()
+        _check(lib().tamc_gla_results(h, _p(pe, f32p), _p(bs, u32p), _p(bd, u32p), _p(be, f32p), C.byref(tot)))
+        st = np.zeros(n.value, np.int8)
+        _check(lib().tamc_gla_state(h, _p(st, i8p)))
+        if output:
+            _check(lib().tamc_gla_write(h, output.encode()))
+    finally:
+        lib().tamc_gla_free(h)
+    return GlaResults(n.value, npart.value, pe, list(zip(bs.tolist(), bd.tolist(), be.tolist())),
+                      np.float32(tot.value), st)
 
 
 # ------------------------------------------------- reference-named runners

@@ -1,10 +1,11 @@
-"""Builds libtamc_b200.so (sm_100a) and the tamc_b200 CLI in-tree.
+"""Builds libtamc_b200.so (sm_100a) and the tamc_b200 / tamc_b200_pt_opt CLIs in-tree.
 
 Steps: generate the glibc-expf exception table (a host C program compared
 against this machine's glibc), embed it with an assembler .incbin, compile the
 C++ host sources with g++ and the CUDA sources with nvcc for sm_100a, link a
 shared library with the static CUDA runtime, then link the CLI against it.
-Outputs: tamc_b200/libtamc_b200.so, tamc_b200/bin/tamc_b200 (object files
+Outputs: tamc_b200/libtamc_b200.so, tamc_b200/bin/tamc_b200 and
+tamc_b200/bin/tamc_b200_pt_opt (object files
 under _build/ at the repository root).
 """
 from __future__ import annotations
@@ -21,14 +22,15 @@ SRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(ROOT, "_build", "tamc_b200")
 LIB = os.path.join(PKG, "libtamc_b200.so")
 CLI = os.path.join(PKG, "bin", "tamc_b200")
+PT_OPT_CLI = os.path.join(PKG, "bin", "tamc_b200_pt_opt")
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
 GXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 GCC = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["ctx.cu", "ref_kernels.cu", "fast_sa.cu", "sa_api.cu", "sa_noalloc.cu", "pt.cu", "fast_pt.cu",
-              "fast_host.cu", "serve.cu"]
-CPP_SOURCES = ["host_instance.cpp", "method.cpp", "writers.cpp"]
+              "fast_host.cu", "serve.cu", "gla.cu"]
+CPP_SOURCES = ["host_instance.cpp", "method.cpp", "writers.cpp", "pt_opt.cpp"]
 HEADERS = ["device.cuh", "expf_exact.h", "internal.h", "fast_common.cuh", "fast_sa.cuh", "fast_pt.cuh", "pt.cuh",
            "ref_kernels.cuh"]
 
@@ -85,12 +87,13 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     # 3. link
     if _newer(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-lpthread", "-ldl", "-lrt"])
-    cli_obj = os.path.join(OUT, "cli.o")
-    cli_src = os.path.join(SRC, "cli.cpp")
-    if _newer(cli_obj, [cli_src] + hdrs):
-        _run([GXX, "-O2", "-std=c++17", "-ffp-contract=off", "-I", SRC, "-c", cli_src, "-o", cli_obj])
-    if _newer(CLI, [cli_obj, LIB]):
-        _run([GXX, "-o", CLI, cli_obj, LIB, "-Wl,-rpath,$ORIGIN/..", "-lpthread"])
+    for src_name, exe in (("cli.cpp", CLI), ("pt_opt_cli.cpp", PT_OPT_CLI)):
+        obj = os.path.join(OUT, src_name + ".o")
+        src = os.path.join(SRC, src_name)
+        if _newer(obj, [src] + hdrs):
+            _run([GXX, "-O2", "-std=c++17", "-ffp-contract=off", "-I", SRC, "-c", src, "-o", obj])
+        if _newer(exe, [obj, LIB]):
+            _run([GXX, "-o", exe, obj, LIB, "-Wl,-rpath,$ORIGIN/..", "-lpthread"])
     if verbose:
         print(f"built {LIB}")
     return LIB

@@ -150,11 +150,38 @@ uint32_t HostInstance::graph_nodes() const {
   bool any = false;
   for (uint32_t i = 0; i < n; ++i)
     for (uint32_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e)
-      if (col[e] != i) {
+      if (col[e] != i || diag_in_graph) {
         any = true;
         mx = std::max(mx, std::max(i, col[e]));
       }
   return any ? mx + 1 : 0;
+}
+
+HostInstance induced_sorted(const HostInstance& h, const std::vector<uint32_t>& nodes) {
+  HostInstance s;
+  s.n = (uint32_t)nodes.size();
+  s.offset = 0.0f;
+  s.diag_in_graph = true;
+  s.row_ptr.assign(1, 0);
+  s.bias.reserve(s.n);
+  for (uint32_t ni : nodes) {
+    s.bias.push_back(h.bias[ni]);
+    for (uint32_t e = h.row_ptr[ni]; e < h.row_ptr[ni + 1]; ++e) {
+      const auto it = std::lower_bound(nodes.begin(), nodes.end(), h.col[e]);
+      if (it != nodes.end() && *it == h.col[e]) {
+        s.col.push_back((uint32_t)(it - nodes.begin()));
+        s.J.push_back(h.J[e]);
+      }
+    }
+    s.row_ptr.push_back((uint32_t)s.col.size());
+  }
+  for (const auto& w : h.suscept) {
+    std::vector<double> sw;
+    sw.reserve(s.n);
+    for (uint32_t ni : nodes) sw.push_back(w[ni]);
+    s.suscept.push_back(std::move(sw));
+  }
+  return s;
 }
 
 bool HostInstance::has_self_loops() const {
@@ -406,3 +433,51 @@ float tamc_instance_energy_ref(const tamc_host_instance* inst, const int8_t* spi
 void tamc_instance_free(tamc_host_instance* inst) { delete inst; }
 
 }  // extern "C"
+
+namespace tamc {
+
+void parse_partition(const char* text, size_t len, uint32_t n, std::vector<std::vector<uint32_t>>& parts) {
+  parts.clear();
+  std::vector<char> in_part(n, 0);
+  const char* p = text;
+  const char* end = text + len;
+  while (p < end) {
+    const char* eol = static_cast<const char*>(memchr(p, '\n', (size_t)(end - p)));
+    if (!eol) eol = end;
+    // one line: many1(delimited(space0, digit1 as u32, multispace0)); a line
+    // without a leading number is skipped, text after the last number ignored
+    std::vector<uint32_t> v;
+    const char* q = p;
+    for (;;) {
+      const char* r = q;
+      while (r < eol && (*r == ' ' || *r == '\t')) ++r;
+      if (r >= eol || *r < '0' || *r > '9') break;
+      uint64_t x = 0;
+      while (r < eol && *r >= '0' && *r <= '9') {
+        x = x * 10 + (uint64_t)(*r - '0');
+        // u32::from_str(..).unwrap() on the digits
+        if (x > 0xffffffffull) fail(TAMC_E_REFPANIC, "partition index does not fit in u32 (the reference panics)");
+        ++r;
+      }
+      while (r < eol && (*r == ' ' || *r == '\t' || *r == '\r')) ++r;
+      v.push_back((uint32_t)x);
+      q = r;
+    }
+    if (!v.empty()) {
+      const uint32_t ip = (uint32_t)parts.size();
+      for (uint32_t i : v) {
+        if (i >= n)
+          fail(TAMC_E_INVAL, "Partitition must be specified for instance size " + std::to_string(n) +
+                                 ". Found index " + std::to_string(i));
+        if (in_part[i])
+          fail(TAMC_E_INVAL, "Index " + std::to_string(i) + " specified more than once in partition " +
+                                 std::to_string(ip));
+        in_part[i] = 1;
+      }
+      parts.push_back(std::move(v));
+    }
+    p = eol + 1;
+  }
+}
+
+}  // namespace tamc

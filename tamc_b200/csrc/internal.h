@@ -47,6 +47,11 @@ struct HostInstance {
   std::vector<float> bias;
   std::vector<std::vector<double>> suscept;
 
+  // The ICM graph's node range also counts self-couplings.  Set on the
+  // sub-instances of a GLA split: their `coupling` matrix is built from every
+  // row entry, the diagonal included (src/ising.rs:327-355).
+  bool diag_in_graph = false;
+
   uint32_t graph_nodes() const;   // petgraph node count of the ICM graph
   bool has_self_loops() const;
   // Colouring of the off-diagonal graph: bipartite 2-colouring when possible,
@@ -56,6 +61,10 @@ struct HostInstance {
 };
 
 void parse_instance_text(const char* text, size_t len, bool qubo, HostInstance& out);
+// induced_subgraph_instance_sorted (src/ising.rs:327-355): the sub-instance on
+// the sorted site list `nodes`, offset 0, rows keep the entries whose column is
+// in `nodes` (renumbered by position), susceptibility weights restricted.
+HostInstance induced_sorted(const HostInstance& h, const std::vector<uint32_t>& nodes);
 std::vector<double> read_txt_vec_file(const std::string& path);
 
 // Method file
@@ -86,9 +95,14 @@ struct SaParamsHost {
   uint32_t num_replicas = 0;
   uint32_t threads = 0;
 };
+struct GlaParamsHost {
+  uint32_t num_threads = 0;
+  std::string partition_file;
+};
 struct Method {
   int kind = 0;
-  PtParamsHost pt;
+  PtParamsHost pt;  // PT, or GLA's pt_params
+  GlaParamsHost gla;
   SaParamsHost sa;
   std::vector<float> betas;  // resolved
   uint32_t lo_beta_idx = 0;
@@ -124,12 +138,29 @@ struct AnnealMinResultsOut {
   std::vector<float> energies;
 };
 std::string yaml_pt_min_results(const PtMinResultsOut& r);
+// serde_yaml of Method::PT(params) (src/lib.rs:80-85), as tamc-pt-opt writes it
+std::string yaml_pt_method(const PtParamsHost& p);
+std::string fmt_f32_display(float v);
 std::string yaml_anneal_min_results(const AnnealMinResultsOut& r);
 std::string bincode_thermal_samples(const ThermalSamplesOut& t);
 std::string bincode_anneal_state(uint32_t instance_size, uint32_t num_replicas, const std::vector<uint8_t>& bytes);
 std::string pickle_thermal_samples(const ThermalSamplesOut& t);
 std::string pickle_anneal_min_results(const AnnealMinResultsOut& r);
 std::string pickle_anneal_state(uint32_t instance_size, uint32_t num_replicas, const std::vector<uint8_t>& bytes);
+// GlaResults (src/gla.rs:61-69)
+struct GlaResultsOut {
+  uint32_t instance_size = 0;
+  uint32_t num_partitions = 0;
+  std::vector<float> partition_energies;
+  std::vector<uint32_t> bnd_src, bnd_dst;
+  std::vector<float> bnd_energies;
+  float total_energy = 0.0f;
+};
+std::string bincode_gla_results(const GlaResultsOut& r);
+std::string pickle_gla_results(const GlaResultsOut& r);
+// read_u32_lines (src/util.rs:142-172) checked as GlaParams::read_graph_partition
+// (src/gla.rs:37-58) for an instance of n sites.
+void parse_partition(const char* text, size_t len, uint32_t n, std::vector<std::vector<uint32_t>>& parts);
 std::string fmt_f32(float v);
 std::string fmt_f64(double v);
 

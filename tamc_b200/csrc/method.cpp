@@ -395,12 +395,9 @@ uint32_t resolve_lo_beta_idx(const PtParamsHost& p, const std::vector<float>& be
   return 0;
 }
 
-void parse_method_yaml(const std::string& text, Method& m) {
-  YNode root = parse_yaml(text);
-  std::string tag;
-  const YNode& body = variant(root, tag, "method");
-  if (tag == "PT") {
-    if (body.kind != YNode::MAP) fail(TAMC_E_PARSE, "PT: expected a mapping");
+// PtIcmParams (src/pt.rs:259-272) from a mapping, with the ladder and lo_beta_idx resolved.
+static void parse_pt_body(const YNode& body, Method& m) {
+  {
     PtParamsHost& p = m.pt;
     p.num_sweeps = get_u32(req(body, "num_sweeps", "PT"), "num_sweeps");
     p.warmup_fraction = get_f64(req(body, "warmup_fraction", "PT"), "warmup_fraction");
@@ -414,12 +411,22 @@ void parse_method_yaml(const std::string& text, Method& m) {
     if (!is_none(v = body.get("sample"))) { p.has_sample = true; p.sample = get_u32(*v, "sample"); }
     if (!is_none(v = body.get("sample_states"))) { p.has_sample_states = true; p.sample_states = get_u32(*v, "sample_states"); }
     if (!is_none(v = body.get("sample_limiting"))) { p.has_sample_limiting = true; p.sample_limiting = get_u8(*v, "sample_limiting"); }
-    m.kind = TAMC_METHOD_PT;
     m.betas = p.beta.resolve();
     for (size_t k = 1; k < m.betas.size(); ++k)
       if (!(m.betas[k] - m.betas[k - 1] >= 0.0f)) fail(TAMC_E_REFPANIC, "beta array must be non-decreasing");
     if (m.betas.empty()) fail(TAMC_E_REFPANIC, "beta array must not be empty");
     m.lo_beta_idx = resolve_lo_beta_idx(p, m.betas, nullptr);
+  }
+}
+
+void parse_method_yaml(const std::string& text, Method& m) {
+  YNode root = parse_yaml(text);
+  std::string tag;
+  const YNode& body = variant(root, tag, "method");
+  if (tag == "PT") {
+    if (body.kind != YNode::MAP) fail(TAMC_E_PARSE, "PT: expected a mapping");
+    parse_pt_body(body, m);
+    m.kind = TAMC_METHOD_PT;
   } else if (tag == "SA") {
     if (body.kind != YNode::MAP) fail(TAMC_E_PARSE, "SA: expected a mapping");
     m.sa.beta = parse_beta(req(body, "beta", "SA"));
@@ -430,6 +437,15 @@ void parse_method_yaml(const std::string& text, Method& m) {
     for (size_t k = 1; k < m.betas.size(); ++k)
       if (!(m.betas[k] - m.betas[k - 1] >= 0.0f)) fail(TAMC_E_REFPANIC, "beta array must be non-decreasing");
   } else if (tag == "GLA") {
+    // GlaParams (src/gla.rs:28-33)
+    if (body.kind != YNode::MAP) fail(TAMC_E_PARSE, "GLA: expected a mapping");
+    m.gla.num_threads = get_u32(req(body, "num_threads", "GLA"), "num_threads");
+    const YNode& pt = req(body, "pt_params", "GLA");
+    if (pt.kind != YNode::MAP) fail(TAMC_E_PARSE, "GLA.pt_params: expected a mapping");
+    parse_pt_body(pt, m);
+    const YNode& pf = req(body, "partition_file", "GLA");
+    if (pf.kind != YNode::SCALAR) fail(TAMC_E_PARSE, "field `partition_file`: expected a string");
+    m.gla.partition_file = pf.s;
     m.kind = TAMC_METHOD_GLA;
   } else {
     fail(TAMC_E_PARSE, "unknown variant `" + tag + "`, expected one of `PT`, `SA`, `GLA`");
@@ -470,10 +486,20 @@ int tamc_method_read(const char* path, tamc_method** out) {
 
 int tamc_method_kind(const tamc_method* m) { return m ? m->m.kind : 0; }
 
+int tamc_method_gla(const tamc_method* m, uint32_t* num_threads, const char** partition_file, tamc_pt_params* p) {
+  TAMC_API_BEGIN
+  if (!m) fail(TAMC_E_INVAL, "null method");
+  if (m->m.kind != TAMC_METHOD_GLA) fail(TAMC_E_INVAL, "not a GLA method");
+  if (num_threads) *num_threads = m->m.gla.num_threads;
+  if (partition_file) *partition_file = m->m.gla.partition_file.c_str();
+  if (p) return tamc_method_pt(m, p);
+  TAMC_API_END
+}
+
 int tamc_method_pt(const tamc_method* m, tamc_pt_params* p) {
   TAMC_API_BEGIN
   if (!m || !p) fail(TAMC_E_INVAL, "null argument");
-  if (m->m.kind != TAMC_METHOD_PT) fail(TAMC_E_INVAL, "not a PT method");
+  if (m->m.kind != TAMC_METHOD_PT && m->m.kind != TAMC_METHOD_GLA) fail(TAMC_E_INVAL, "not a PT method");
   const PtParamsHost& q = m->m.pt;
   p->num_sweeps = q.num_sweeps;
   p->warmup_fraction = q.warmup_fraction;

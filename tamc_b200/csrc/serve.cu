@@ -9,11 +9,13 @@
 // Every request runs exactly the Markov chain it would run alone: its Philox
 // streams depend only on its own seed and sweep index, and its state is only
 // touched by the CTA that owns it during a launch.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
 #include <deque>
 #include <map>
+#include <string>
 
 #include "fast_pt.cuh"
 
@@ -39,7 +41,8 @@ struct Request {
   uint64_t footprint = 0;
   tamc_inst* dinst = nullptr;
   tamc_pt* pt = nullptr;
-  int state = 0;  // 0 queued, 1 active, 2 done
+  int state = 0;  // TAMC_REQ_QUEUED / _ACTIVE / _DONE / _CANCELLED / _FAILED
+  std::string error;  // why admission failed
   Clock::time_point t_submit, t_done;
   float best = INFINITY;
   uint32_t sweeps = 0;
@@ -83,7 +86,10 @@ struct tamc_server {
   }
 };
 
-static void retire(tamc_server* s, Request* r) {
+// Ends an active request: its final replicas and energies are copied out,
+// its device state freed and its HBM budget returned.  `state` is
+// TAMC_REQ_DONE, or TAMC_REQ_CANCELLED for a request stopped between steps.
+static void retire(tamc_server* s, Request* r, int state = TAMC_REQ_DONE) {
   const uint32_t n = r->h->h.n;
   const size_t R = (size_t)r->p.num_replica_chains * r->p.num_beta;
   r->final_spins.resize(R * n);
@@ -95,7 +101,7 @@ static void retire(tamc_server* s, Request* r) {
   tamc_gpu_instance_destroy(r->dinst);
   r->pt = nullptr;
   r->dinst = nullptr;
-  r->state = 2;
+  r->state = state;
   r->t_done = Clock::now();
   s->used -= r->footprint;
 }
@@ -150,17 +156,32 @@ int tamc_serve_step(tamc_server* s, uint32_t* active, uint32_t* queued) {
   if (!s) fail(TAMC_E_INVAL, "null server");
   TAMC_CUDA(cudaSetDevice(s->g->device));
   // admission: FIFO while slots and HBM budget allow
+  // A request that cannot be set up (its instance or run is refused) fails
+  // alone: it is marked TAMC_REQ_FAILED with the reason and the others go on.
   while (!s->queue.empty() && s->active.size() < s->max_active && s->used + s->queue.front()->footprint <= s->budget) {
     Request* r = s->queue.front();
     s->queue.pop_front();
     int rc = tamc_gpu_instance_upload(s->g, r->h, &r->dinst);
-    if (rc != TAMC_OK) fail(rc, tamc_last_error());
-    g_no_autotune = true;
-    rc = tamc_gpu_pt_create(r->dinst, &r->p, r->seed, TAMC_MODE_FAST, &r->pt);
-    g_no_autotune = false;
-    if (rc != TAMC_OK) fail(rc, tamc_last_error());
-    if (r->pt->fast && r->pt->fast_plain()) fail(TAMC_E_UNSUPPORTED, "request too large for the fused PT kernel");
-    r->state = 1;
+    if (rc == TAMC_OK) {
+      g_no_autotune = true;
+      rc = tamc_gpu_pt_create(r->dinst, &r->p, r->seed, TAMC_MODE_FAST, &r->pt);
+      g_no_autotune = false;
+    }
+    if (rc == TAMC_OK && r->pt->fast && r->pt->fast_plain()) {
+      rc = TAMC_E_UNSUPPORTED;
+      set_error("request too large for the fused PT kernel");
+    }
+    if (rc != TAMC_OK) {
+      r->error = tamc_last_error();
+      if (r->pt) tamc_gpu_pt_destroy(r->pt);
+      if (r->dinst) tamc_gpu_instance_destroy(r->dinst);
+      r->pt = nullptr;
+      r->dinst = nullptr;
+      r->state = TAMC_REQ_FAILED;
+      r->t_done = Clock::now();
+      continue;
+    }
+    r->state = TAMC_REQ_ACTIVE;
     s->used += r->footprint;
     s->active.push_back(r);
   }
@@ -173,7 +194,7 @@ int tamc_serve_step(tamc_server* s, uint32_t* active, uint32_t* queued) {
       const auto& E = r->pt->out.h_E;
       if (!E.empty()) r->best = E.back();
       const bool hit = !std::isnan(r->target) && r->best <= r->target;
-      if (r->pt->next_sweep >= r->pt->cfg.num_sweeps || hit) retire(s, r);
+      if (r->pt->next_sweep >= r->pt->cfg.num_sweeps || hit) retire(s, r, TAMC_REQ_DONE);
       else keep.push_back(r);
     }
     s->active.swap(keep);
@@ -190,11 +211,42 @@ int tamc_serve_result(tamc_server* s, uint64_t request_id, int32_t* done, float*
   auto it = s->all.find(request_id);
   if (it == s->all.end()) fail(TAMC_E_INVAL, "no such request");
   Request* r = it->second;
-  if (done) *done = r->state == 2;
+  const bool ended = r->state >= TAMC_REQ_DONE;
+  if (done) *done = ended;
   if (best_energy) *best_energy = r->best;
-  if (sweeps) *sweeps = r->state == 2 ? r->sweeps : (r->pt ? r->pt->next_sweep : 0);
-  if (latency_s)
-    *latency_s = r->state == 2 ? std::chrono::duration<double>(r->t_done - r->t_submit).count() : -1.0;
+  if (sweeps) *sweeps = ended ? r->sweeps : (r->pt ? r->pt->next_sweep : 0);
+  if (latency_s) *latency_s = ended ? std::chrono::duration<double>(r->t_done - r->t_submit).count() : -1.0;
+  TAMC_API_END
+}
+
+int tamc_serve_status(tamc_server* s, uint64_t request_id, int32_t* status, const char** error) {
+  TAMC_API_BEGIN
+  if (!s) fail(TAMC_E_INVAL, "null server");
+  auto it = s->all.find(request_id);
+  if (it == s->all.end()) fail(TAMC_E_INVAL, "no such request");
+  if (status) *status = it->second->state;
+  if (error) *error = it->second->error.c_str();
+  TAMC_API_END
+}
+
+int tamc_serve_cancel(tamc_server* s, uint64_t request_id) {
+  TAMC_API_BEGIN
+  if (!s) fail(TAMC_E_INVAL, "null server");
+  auto it = s->all.find(request_id);
+  if (it == s->all.end()) fail(TAMC_E_INVAL, "no such request");
+  Request* r = it->second;
+  if (r->state == TAMC_REQ_QUEUED) {
+    s->queue.erase(std::find(s->queue.begin(), s->queue.end(), r));
+    r->state = TAMC_REQ_CANCELLED;
+    r->t_done = Clock::now();
+  } else if (r->state == TAMC_REQ_ACTIVE) {
+    // steps run synchronously: between calls no launch of this request is in flight
+    TAMC_CUDA(cudaSetDevice(s->g->device));
+    s->active.erase(std::find(s->active.begin(), s->active.end(), r));
+    retire(s, r, TAMC_REQ_CANCELLED);
+  } else {
+    fail(TAMC_E_INVAL, "request already ended");
+  }
   TAMC_API_END
 }
 
@@ -204,7 +256,8 @@ int tamc_serve_state(tamc_server* s, uint64_t request_id, int8_t* spins, float* 
   auto it = s->all.find(request_id);
   if (it == s->all.end()) fail(TAMC_E_INVAL, "no such request");
   Request* r = it->second;
-  if (r->state != 2) fail(TAMC_E_INVAL, "request not retired yet");
+  if (r->state != TAMC_REQ_DONE && r->state != TAMC_REQ_CANCELLED) fail(TAMC_E_INVAL, "request not retired yet");
+  if (r->final_spins.empty()) fail(TAMC_E_INVAL, "request ended before it ran (cancelled in the queue or failed)");
   if (spins) memcpy(spins, r->final_spins.data(), r->final_spins.size());
   if (energies) memcpy(energies, r->final_energies.data(), r->final_energies.size() * 4);
   TAMC_API_END

@@ -53,6 +53,35 @@ static std::string fmt_shortest(double v, bool is_f32) {
   return neg ? "-" + out : out;
 }
 std::string fmt_f32(float v) { return fmt_shortest((double)v, true); }
+
+// Rust's Display of an f32 (`{}`): the shortest round-trip digits written out
+// in positional notation, with no `.0` on whole numbers.
+std::string fmt_f32_display(float v) {
+  if (std::isnan(v)) return "NaN";
+  if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
+  if (v == 0.0f) return std::signbit(v) ? "-0" : "0";
+  char buf[64];
+  int prec = 1;
+  for (; prec <= 9; ++prec) {
+    snprintf(buf, sizeof buf, "%.*e", prec - 1, (double)v);
+    if (strtof(buf, nullptr) == v) break;
+  }
+  std::string s(buf);
+  const bool neg = s[0] == '-';
+  if (neg) s = s.substr(1);
+  const size_t epos = s.find('e');
+  const int exp10 = atoi(s.c_str() + epos + 1);
+  std::string digits;
+  for (size_t k = 0; k < epos; ++k)
+    if (s[k] != '.') digits += s[k];
+  while (digits.size() > 1 && digits.back() == '0') digits.pop_back();
+  const int len = (int)digits.size(), kk = exp10 + 1;
+  std::string out;
+  if (kk <= 0) out = "0." + std::string((size_t)(-kk), '0') + digits;
+  else if (kk >= len) out = digits + std::string((size_t)(kk - len), '0');
+  else out = digits.substr(0, (size_t)kk) + "." + digits.substr((size_t)kk);
+  return neg ? "-" + out : out;
+}
 std::string fmt_f64(double v) { return fmt_shortest(v, false); }
 
 namespace {
@@ -86,22 +115,35 @@ void yaml_beta(Y& y, int ind, const BetaSpec& b) {
 }
 }  // namespace
 
+// PtIcmParams fields (src/pt.rs:259-272) at indentation `ind`
+static void yaml_pt_params(Y& y, int ind, const PtParamsHost& p) {
+  y.kv(ind, "num_sweeps", std::to_string(p.num_sweeps));
+  y.kv(ind, "warmup_fraction", fmt_f64(p.warmup_fraction));
+  yaml_beta(y, ind, p.beta);
+  y.kv(ind, "lo_beta", p.has_lo_beta ? fmt_f32(p.lo_beta) : "~");
+  y.kv(ind, "lo_num_beta", p.has_lo_num_beta ? std::to_string(p.lo_num_beta) : "~");
+  y.kv(ind, "icm", p.icm ? "true" : "false");
+  y.kv(ind, "num_replica_chains", std::to_string(p.num_replica_chains));
+  y.kv(ind, "threads", std::to_string(p.threads));
+  y.kv(ind, "sample", p.has_sample ? std::to_string(p.sample) : "~");
+  y.kv(ind, "sample_states", p.has_sample_states ? std::to_string(p.sample_states) : "~");
+  y.kv(ind, "sample_limiting", p.has_sample_limiting ? std::to_string(p.sample_limiting) : "~");
+}
+
+std::string yaml_pt_method(const PtParamsHost& p) {
+  Y y;
+  y.o = "---\n";
+  y.key(0, "PT");
+  yaml_pt_params(y, 2, p);
+  return y.o;
+}
+
 std::string yaml_pt_min_results(const PtMinResultsOut& r) {
   Y y;
   y.o = "---\n";
   const PtParamsHost& p = *r.params;
   y.key(0, "params");
-  y.kv(2, "num_sweeps", std::to_string(p.num_sweeps));
-  y.kv(2, "warmup_fraction", fmt_f64(p.warmup_fraction));
-  yaml_beta(y, 2, p.beta);
-  y.kv(2, "lo_beta", p.has_lo_beta ? fmt_f32(p.lo_beta) : "~");
-  y.kv(2, "lo_num_beta", p.has_lo_num_beta ? std::to_string(p.lo_num_beta) : "~");
-  y.kv(2, "icm", p.icm ? "true" : "false");
-  y.kv(2, "num_replica_chains", std::to_string(p.num_replica_chains));
-  y.kv(2, "threads", std::to_string(p.threads));
-  y.kv(2, "sample", p.has_sample ? std::to_string(p.sample) : "~");
-  y.kv(2, "sample_states", p.has_sample_states ? std::to_string(p.sample_states) : "~");
-  y.kv(2, "sample_limiting", p.has_sample_limiting ? std::to_string(p.sample_limiting) : "~");
+  yaml_pt_params(y, 2, p);
   y.kv(0, "timing", fmt_f64(r.timing_us));
   y.seq(0, "gs_time_steps", r.gs_time_steps, [](uint32_t v) { return std::to_string(v); });
   y.seq(0, "gs_energies", r.gs_energies, [](float v) { return fmt_f32(v); });
@@ -230,6 +272,8 @@ struct Pk {
   void dict_end() { o.push_back('u'); }
   void list_begin() { o.push_back(']'); o.push_back('('); }
   void list_end() { o.push_back('e'); }
+  void tuple_begin() { o.push_back('('); }
+  void tuple_end() { o.push_back('t'); }
   std::string finish() { o.push_back('.'); return o; }
 };
 
@@ -302,6 +346,48 @@ std::string pickle_anneal_state(uint32_t instance_size, uint32_t num_replicas, c
   p.str("instance_size"); p.u64(instance_size);
   p.str("num_replicas"); p.u64(num_replicas);
   p.str("bytes"); p.list_begin(); for (uint8_t b : bytes) p.u64(b); p.list_end();
+  p.dict_end();
+  return p.finish();
+}
+
+// GlaResults (src/gla.rs:61-69) in bincode's default encoding: instance_size
+// u32, num_partitions u32, partition_energies Vec<f32>, boundary_energies
+// Vec<(u32, u32, f32)>, final_state Vec<u8> (left empty by run_gla), total_energy f32.
+std::string bincode_gla_results(const GlaResultsOut& r) {
+  B b;
+  b.u32(r.instance_size);
+  b.u32(r.num_partitions);
+  b.len(r.partition_energies.size());
+  for (float v : r.partition_energies) b.f32(v);
+  b.len(r.bnd_energies.size());
+  for (size_t k = 0; k < r.bnd_energies.size(); ++k) {
+    b.u32(r.bnd_src[k]);
+    b.u32(r.bnd_dst[k]);
+    b.f32(r.bnd_energies[k]);
+  }
+  b.len(0);
+  b.f32(r.total_energy);
+  return b.o;
+}
+
+std::string pickle_gla_results(const GlaResultsOut& r) {
+  Pk p;
+  p.dict_begin();
+  p.str("instance_size"); p.u64(r.instance_size);
+  p.str("num_partitions"); p.u64(r.num_partitions);
+  p.str("partition_energies"); p.list_begin(); for (float v : r.partition_energies) p.f64(v); p.list_end();
+  p.str("boundary_energies");
+  p.list_begin();
+  for (size_t k = 0; k < r.bnd_energies.size(); ++k) {
+    p.tuple_begin();
+    p.u64(r.bnd_src[k]);
+    p.u64(r.bnd_dst[k]);
+    p.f64(r.bnd_energies[k]);
+    p.tuple_end();
+  }
+  p.list_end();
+  p.str("final_state"); p.list_begin(); p.list_end();
+  p.str("total_energy"); p.f64(r.total_energy);
   p.dict_end();
   return p.finish();
 }

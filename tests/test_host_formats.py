@@ -203,3 +203,81 @@ def test_ref_expf_matches_glibc(tb):
     bad = [x for x in xs if np.float32(L.tamc_ref_expf(float(x))).view(np.uint32)
            != np.float32(libm.expf(float(x))).view(np.uint32)]
     assert not bad, bad[:5]
+
+
+def _py_read_u32_lines(text):
+    """read_u32_lines (src/util.rs:142-172) restated: per line, whitespace-separated
+    leading u32 values (space0 before, multispace0 after each), the rest ignored;
+    lines without a leading value skipped."""
+    out = []
+    for line in text.split("\n"):
+        if line.endswith("\r"):
+            line = line[:-1]  # BufRead::lines strips "\r\n"
+        vals, k = [], 0
+        while True:
+            j = k
+            while j < len(line) and line[j] in " \t":
+                j += 1
+            m = j
+            while m < len(line) and line[m].isdigit() and line[m].isascii():
+                m += 1
+            if m == j:
+                break
+            vals.append(int(line[j:m]))
+            while m < len(line) and line[m] in " \t\r\n":
+                m += 1
+            k = m
+        if vals:
+            out.append(vals)
+    return out
+
+
+@pytest.mark.parametrize("text", [
+    "0 1 2\n3 4 5\n",
+    "  0\t1  \r\n2 3 4\r\n\n\n5\n",
+    "0 1 x 9\n# comment 2\n2,3\n4 5",
+    "5 4 3\n\n2 1 0 \n",
+    "",
+])
+def test_partition_parse_matches_restatement(tb, text):
+    p = tb.Partition.parse(text, 10)
+    assert p.parts == _py_read_u32_lines(text)
+
+
+def test_partition_errors_follow_read_graph_partition(tb):
+    with pytest.raises(tb.TamcError) as e:
+        tb.Partition.parse("0 1\n2 10\n", 10)
+    assert e.value.code == -1 and "Found index 10" in str(e.value)
+    with pytest.raises(tb.TamcError) as e:
+        tb.Partition.parse("0 1\n2 1\n", 10)
+    assert e.value.code == -1 and "Index 1 specified more than once in partition 1" in str(e.value)
+    with pytest.raises(tb.TamcError) as e:  # u32::from_str(..).unwrap() panics
+        tb.Partition.parse("0 99999999999\n", 10)
+    assert e.value.code == -8
+    with pytest.raises(tb.TamcError) as e:
+        tb.Partition.read("/nonexistent/parts.txt", 10)
+    assert e.value.code == -6
+
+
+def test_gla_method_file(tb):
+    m = tb.Method.parse("""GLA:
+  num_threads: 6
+  pt_params:
+    num_sweeps: 100
+    warmup_fraction: 0.25
+    beta:
+      Arr: [0.1, 0.5, 1.0, 2.0]
+    lo_num_beta: 2
+    icm: true
+    num_replica_chains: 4
+    threads: 3
+    sample: 10
+  partition_file: "parts/p.txt"
+""")
+    assert m.kind == "GLA"
+    nt, pf, p = m.gla()
+    assert nt == 6 and pf == "parts/p.txt"
+    assert p.num_sweeps == 100 and p.lo_beta_idx == 2 and p.num_replica_chains == 4 and p.sample == 10
+    assert np.array_equal(p.betas, np.array([0.1, 0.5, 1.0, 2.0], np.float32))
+    with pytest.raises(tb.TamcError):
+        tb.Method.parse("GLA:\n  num_threads: 1\n  partition_file: x\n")  # pt_params missing
