@@ -334,9 +334,10 @@ def run_c3(args):
     lib_stream = torch.cuda.ExternalStream(gpu.stream, device=dev)
     jobs = c3_jobs(rank)
     hosts = [tb.HostInstance.parse(gi.lattice(L, 2, "pm", si)) for L, _, si, _ in jobs]
-    params = [_lattice_params(tb, nt, C3_SWEEPS) for _, nt, _, _ in jobs]
+    sweeps = args.c3_sweeps
+    params = [_lattice_params(tb, nt, sweeps) for _, nt, _, _ in jobs]
     dinsts = [gpu.upload(h) for h in hosts]
-    flips = c3_flips(jobs)
+    flips = c3_flips(jobs, sweeps)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def make_batch(k):
@@ -417,7 +418,7 @@ def run_c3(args):
         clocks = clk.summary()
         peak, kind = _peaks()
         dev_ms_step = dev_ms / args.steps
-        bytes_step = c3_bytes(jobs)
+        bytes_step = c3_bytes(jobs, sweeps)
         achieved = bytes_step / (dev_ms_step / 1e3) / 1e9
         traffic = _profile_value("pt_fused_c3.md", "dram_bytes_per_step")
         inst = _profile_value("pt_fused_c3.md", "warp_instructions_per_step")
@@ -432,7 +433,7 @@ def run_c3(args):
         out = {"metric": METRIC, "value": value, "unit": "flips/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": float(ms_t.item()) / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-               "config": C3_CONFIG,
+               "config": C3_CONFIG if sweeps == C3_SWEEPS else dict(C3_CONFIG, sweeps=sweeps),
                "flips_per_step": flips,
                "e2e": {"value": e2e_value, "unit": "flips/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(d2h),
@@ -447,7 +448,7 @@ def run_c3(args):
                "issue_roofline": issue,
                "clocks": clocks, "best_energy_jobs_0_3": best}
         if world == 1 and args.c3_plain > 0:
-            out.update(c3_plain(args, tb, gpu, lib_stream, jobs, dinsts, params, value))
+            out.update(c3_plain(args, tb, gpu, lib_stream, jobs, dinsts, params, value, sweeps))
         if world == 1 and not args.no_cpu:
             cpu = _child_json(["--cpu-leg", "c3", "--cpu-stride", str(args.cpu_stride), "--cpu-runs", "3"])
             out["cpu_baseline"] = {"value": cpu["value"], "unit": "flips/s", "cores": cpu["cores"], "kind": "port",
@@ -465,7 +466,7 @@ def run_c3(args):
     return 0
 
 
-def c3_plain(args, tb, gpu, lib_stream, jobs, dinsts, params, batched):
+def c3_plain(args, tb, gpu, lib_stream, jobs, dinsts, params, batched, sweeps):
     """The plain form on jobs 0, s, 2s, ... (s = 256 / --c3-plain): one run at a
     time, CUDA events around each run's sweep loop."""
     import torch
@@ -485,7 +486,7 @@ def c3_plain(args, tb, gpu, lib_stream, jobs, dinsts, params, batched):
             e1.synchronize()
             ms += e0.elapsed_time(e1)
             L, nt = jobs[k][0], jobs[k][1]
-            f += L * L * nt * 2 * C3_SWEEPS
+            f += L * L * nt * 2 * sweeps
             del r
     finally:
         del os.environ["TAMC_PT_FORM"]
@@ -778,6 +779,7 @@ def main():
     ap.add_argument("--no-c4", action="store_true", help="skip the C4 keys of the default line")
     ap.add_argument("--workload", default="batch_c3", choices=["batch_c3", "sa_c2", "pt_c1", "pt_c4", "serve_c5"])
     ap.add_argument("--c3-plain", type=int, default=64, help="jobs of the plain-form comparison (0 skips it)")
+    ap.add_argument("--c3-sweeps", type=int, default=C3_SWEEPS, help="sweeps per job (profiling runs only)")
     ap.add_argument("--c4-sweeps", type=int, default=20000)
     ap.add_argument("--c4-cpu-sweeps", type=int, default=1000)
     ap.add_argument("--c5-requests", type=int, default=1000)

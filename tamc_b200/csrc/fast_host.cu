@@ -276,7 +276,8 @@ static void plain_enqueue_rounds(tamc_pt* pt, uint32_t K) {
   const auto& off = pt->inst->color_off;
   for (uint32_t r = 0; r < K; ++r) {
     plain_launch_head(st, F->d_job.p, F->ctl.p, F->eacc.p, 1, F->head_smem, F->head_stage);
-    if (!plain_launch_icm(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, pt->g->smem_optin, F->dm.p))
+    if (!plain_launch_icm(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, pt->g->smem_optin,
+                          (uint32_t)pt->g->num_sms, F->dm.p))
       plain_launch_exch(st, j, F->d_job.p, F->ctl.p, F->icm_dE.p, F->icm_valid.p, F->dm.p);
     plain_launch_perm(st, j, F->d_job.p, F->dm.p, F->grid_cap);
     for (uint32_t c = 0; c + 1 < off.size(); ++c)

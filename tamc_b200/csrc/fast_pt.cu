@@ -26,7 +26,10 @@
 //     measurements and bit-packed state snapshots (src/pt.rs:167-226, 542-583).
 #include "fast_pt.cuh"
 
+#include <cooperative_groups.h>
 #include <numeric>
+
+namespace cg = cooperative_groups;
 
 namespace tamc {
 namespace {
@@ -1354,6 +1357,8 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
   load_job(s_J, jp);
   const PtJob& J = s_J;
   const uint32_t tid = threadIdx.x;
+  // rounds without measurements were closed by the last sweep launch
+  if (mode != 2 && !ctl->pending) return;
   char* base = reinterpret_cast<char*>(smem_u4);
   Smem S{};
   S.Ec = (double*)base;
@@ -1500,6 +1505,270 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__
   plain_exchange_body(J, ctl, icm_dE, icm_valid, base, dm);
 }
 
+// Houdayer moves of round ctl->i on thread-block clusters: one cluster of CL
+// CTAs per (chain pair, slot >= lo), each CTA owning the sites of one
+// contiguous colour-order range (on square and cubic lattices a slab of the
+// lattice).  Every CTA keeps full copies of the disagreement words XD, the
+// cluster words XC and replica 0's words R0 in its shared memory; a site's
+// owner updates it and, when a neighbour lives in another range, stores the
+// new word into the other CTAs' copies through distributed shared memory.
+//   seed    each CTA counts the q<0 sites of its range (ballots), the counts
+//           are exchanged, and the CTA holding the k-th site in colour order
+//           (the rule of icm_group) publishes it;
+//   growth  in-place propagation passes (icm_group's rule C[s] |= D[s] & OR_j C[j],
+//           the site state and columns in registers), a cluster barrier per
+//           pass, each CTA's "grew" flag stored into every CTA before it;
+//   apply   each CTA sums the boundary terms of its cluster sites (fixed
+//           point, integer sums) and flips them; CTA 0 adds the partial sums.
+// The cluster is the exact component of the seed, the sums are integers, so
+// the result equals the one-CTA kernel's bit for bit.  Rows of DEG entries
+// (uniform degree); at most PS sites per thread and range.
+struct IcmClScratch {
+  uint32_t *XD, *XC, *R0;
+  uint16_t* cols;          // [PS * T][DEG] columns of this CTA's sites
+  uint32_t* cnt;           // [CL] q<0 counts per range
+  uint32_t* seed;          // [1]
+  uint32_t* flags;         // [2][CL] per-pass "grew" flags, by pass parity
+  long long* part;         // [CL] partial energy sums (in CTA 0)
+  long long* wsum;         // [32] per-warp sums
+  uint32_t* wcnt;          // [32] per-warp counts
+};
+__host__ __device__ inline size_t carve_icm_cl(IcmClScratch* X, char* base, uint32_t n, uint32_t T, uint32_t PS,
+                                               uint32_t DEG, uint32_t CL) {
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    char* p = base ? base + o : nullptr;
+    o = al16(o + bytes);
+    return p;
+  };
+  char* XD = take((size_t)n * 4);
+  char* XC = take((size_t)n * 4);
+  char* R0 = take((size_t)n * 4);
+  char* cols = take((size_t)PS * T * DEG * 2);
+  char* cnt = take((size_t)CL * 4);
+  char* seed = take(4);
+  char* flags = take((size_t)2 * CL * 4);
+  char* part = take((size_t)CL * 8);
+  char* wsum = take(32 * 8);
+  char* wcnt = take(32 * 4);
+  if (X) {
+    X->XD = (uint32_t*)XD;
+    X->XC = (uint32_t*)XC;
+    X->R0 = (uint32_t*)R0;
+    X->cols = (uint16_t*)cols;
+    X->cnt = (uint32_t*)cnt;
+    X->seed = (uint32_t*)seed;
+    X->flags = (uint32_t*)flags;
+    X->part = (long long*)part;
+    X->wsum = (long long*)wsum;
+    X->wcnt = (uint32_t*)wcnt;
+  }
+  return o;
+}
+
+template <uint32_t CL, uint32_t DEG, uint32_t PS>
+__global__ void __launch_bounds__(1024, 1) k_plain_icm_cl(const PtJob* __restrict__ jp, PlainCtl* ctl,
+                                                          long long* icm_dE, uint32_t* icm_valid,
+                                                          unsigned long long* dm) {
+  extern __shared__ uint4 smem_u4[];
+  __shared__ PtJob s_J;
+  load_job(s_J, jp);
+  const PtJob& J = s_J;
+  cg::cluster_group cluster = cg::this_cluster();
+  const uint32_t r = cluster.block_rank();
+  const uint32_t tid = threadIdx.x, T = blockDim.x, lane = tid & 31u, warp = tid >> 5, nwarp = T >> 5;
+  const uint32_t n = J.n, nw = J.nw, nact = J.nt - J.lo;
+  const uint32_t cid = blockIdx.x / CL;
+  const uint32_t p = cid / nact, t = J.lo + cid % nact;
+  const uint32_t b = t & 31u, bit = 1u << b, w = t >> 5;
+  const uint32_t o0 = 2 * p * J.wpc + w, o1 = (2 * p + 1) * J.wpc + w;
+  const uint32_t i = ctl->i;
+  char* base = reinterpret_cast<char*>(smem_u4);
+  IcmClScratch X;
+  carve_icm_cl(&X, base, n, T, PS, DEG, CL);
+  const uint32_t span = (n + CL - 1) / CL;
+  const uint32_t lo = min(n, r * span), hi = min(n, lo + span);
+  uint32_t* const W = J.W;
+  PhaseClock pc;
+  pc.start(r == 0 ? J.prof : nullptr);
+  // full copies of the disagreement and replica-0 words; columns of own sites
+  for (uint32_t s = tid; s < n; s += T) {
+    const uint32_t v0 = W[s * nw + o0], v1 = W[s * nw + o1];
+    X.XD[s] = (v0 ^ v1) & bit;
+    X.R0[s] = v0;
+    X.XC[s] = 0;
+  }
+  for (uint32_t x = tid; x < (hi - lo) * DEG; x += T) X.cols[x] = J.F.col16[lo * DEG + x];
+  if (tid < 2 * CL) X.flags[tid] = 0;
+  __syncthreads();
+  cluster.sync();  // every CTA of the cluster has started and cleared its copies
+  // ---- seed: q<0 counts of every range, then the k-th site in colour order
+  const uint32_t seg = ((hi - lo + nwarp - 1) / nwarp + 31u) & ~31u;
+  const uint32_t w0 = min(hi, lo + warp * seg), w1 = min(hi, w0 + seg);
+  uint32_t wc = 0;
+  for (uint32_t s0 = w0; s0 < w1; s0 += 32) {
+    const uint32_t s = s0 + lane;
+    wc += __popc(__ballot_sync(0xffffffffu, s < w1 && X.XD[s]));
+  }
+  if (lane == 0) X.wcnt[warp] = wc;
+  __syncthreads();
+  const uint32_t v = lane < nwarp ? X.wcnt[lane] : 0u;
+  uint32_t incl = v;
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= (uint32_t)off) incl += y;
+  }
+  const uint32_t cnt_r = __shfl_sync(0xffffffffu, incl, 31);
+  const uint32_t before_w = __shfl_sync(0xffffffffu, incl - v, warp);
+  if (tid == 0)
+    for (uint32_t q = 0; q < CL; ++q) cluster.map_shared_rank(X.cnt, q)[r] = cnt_r;
+  cluster.sync();
+  uint32_t total = 0, before_r = 0;
+  for (uint32_t q = 0; q < CL; ++q) {
+    const uint32_t c = X.cnt[q];
+    if (q < r) before_r += c;
+    total += c;
+  }
+  if (total) {
+    const uint32_t u = philox4x32_10(make_uint4(32 * w + b, i, p, PTAG_ICM), J.key).x;
+    const uint32_t k = (uint32_t)(((uint64_t)u * total) >> 32);
+    const uint32_t kb = before_r + before_w;
+    if (k >= kb && k < kb + wc) {
+      uint32_t rem = k - kb;
+      for (uint32_t s0 = w0; s0 < w1; s0 += 32) {
+        const uint32_t s = s0 + lane;
+        const uint32_t bal = __ballot_sync(0xffffffffu, s < w1 && X.XD[s]);
+        const uint32_t c = __popc(bal);
+        if (rem < c) {
+          if (lane == 0) {
+            const uint32_t sd = s0 + __fns(bal, 0, (int)rem + 1);
+            for (uint32_t q = 0; q < CL; ++q) *cluster.map_shared_rank(X.seed, q) = sd;
+          }
+          break;
+        }
+        rem -= c;
+      }
+    }
+  }
+  cluster.sync();
+  pc.lap(PHASE_ICM_SCAN);
+  if (total) {
+    if (tid == 0) X.XC[*X.seed] = bit;
+    __syncthreads();
+    // ---- growth: propagation passes over this CTA's sites
+    // two 16-bit columns per register
+    constexpr uint32_t NP = DEG / 2;
+    uint32_t d[PS], c[PS], jp[PS][NP];
+    bool edge[PS];
+#pragma unroll
+    for (uint32_t k = 0; k < PS; ++k) {
+      const uint32_t s = lo + tid + k * T;
+      d[k] = 0;
+      c[k] = 0;
+      edge[k] = false;
+#pragma unroll
+      for (uint32_t m = 0; m < NP; ++m) jp[k][m] = 0;
+      if (s < hi) {
+        d[k] = X.XD[s];
+        c[k] = X.XC[s];
+#pragma unroll
+        for (uint32_t m = 0; m < NP; ++m) {
+          const uint32_t ja = X.cols[(s - lo) * DEG + 2 * m], jb = X.cols[(s - lo) * DEG + 2 * m + 1];
+          jp[k][m] = ja | (jb << 16);
+          edge[k] |= ja < lo || ja >= hi || jb < lo || jb >= hi;
+        }
+      }
+    }
+    for (uint32_t pass = 0; pass < 32u * n + 2u; ++pass) {
+      int grew = 0;
+#pragma unroll
+      for (uint32_t k = 0; k < PS; ++k) {
+        if ((c[k] & d[k]) == d[k]) continue;
+        uint32_t nb = 0;
+#pragma unroll
+        for (uint32_t m = 0; m < NP; ++m) nb |= X.XC[jp[k][m] & 0xffffu] | X.XC[jp[k][m] >> 16];
+        const uint32_t nc = c[k] | (nb & d[k]);
+        if (nc != c[k]) {
+          const uint32_t s = lo + tid + k * T;
+          c[k] = nc;
+          X.XC[s] = nc;
+          grew = 1;
+          if (edge[k])
+            for (uint32_t q = 0; q < CL; ++q)
+              if (q != r) cluster.map_shared_rank(X.XC, q)[s] = nc;
+        }
+      }
+      const int any_cta = __syncthreads_or(grew);
+      const uint32_t par = pass & 1u;
+      if (tid == 0) {
+        if (any_cta)
+          for (uint32_t q = 0; q < CL; ++q) cluster.map_shared_rank(X.flags, q)[par * CL + r] = 1u;
+        for (uint32_t q = 0; q < CL; ++q) X.flags[(par ^ 1u) * CL + q] = 0u;  // written no earlier than next pass
+      }
+      cluster.sync();
+      uint32_t any = 0;
+      for (uint32_t q = 0; q < CL; ++q) any |= X.flags[par * CL + q];
+      if (!any) break;
+    }
+  }
+  pc.lap(PHASE_ICM_GROW);
+  // ---- energy change of the flip (replica 0; replica 1's is its negative) and the flip
+  long long a0 = 0;
+  if (total) {
+    const uint2* __restrict__ ent = J.F.ent;
+    const float* __restrict__ bias = J.F.bias;
+    for (uint32_t s = lo + tid; s < hi; s += T) {
+      if (!(X.XC[s] & bit)) continue;
+      float f0 = bias[s];
+      uint2 ce[DEG];
+#pragma unroll
+      for (uint32_t m = 0; m < DEG; ++m) ce[m] = ent[s * DEG + m];
+#pragma unroll
+      for (uint32_t m = 0; m < DEG; ++m) {
+        if (ce[m].x == s || (X.XC[ce[m].x] & bit)) continue;
+        const float Jv = __uint_as_float(ce[m].y);
+        f0 += (X.R0[ce[m].x] & bit) ? -Jv : Jv;
+      }
+      const float s0 = (X.R0[s] & bit) ? -1.0f : 1.0f;
+      a0 += to_fx(-2.0f * s0 * f0);
+      atomicXor(&W[s * nw + o0], bit);
+      atomicXor(&W[s * nw + o1], bit);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+  if (lane == 0) X.wsum[warp] = a0;
+  __syncthreads();
+  if (tid == 0) {
+    long long sum = 0;
+    for (uint32_t k = 0; k < nwarp; ++k) sum += X.wsum[k];
+    cluster.map_shared_rank(X.part, 0)[r] = sum;
+  }
+  cluster.sync();  // the last access to another CTA's shared memory
+  if (r == 0 && tid == 0) {
+    long long sum = 0;
+    for (uint32_t q = 0; q < CL; ++q) sum += X.part[q];
+    const uint32_t x0 = 2 * p * J.ntp + t, x1 = (2 * p + 1) * J.ntp + t;
+    const uint32_t valid = total != 0;
+    icm_valid[x0] = valid;
+    icm_valid[x1] = valid;
+    icm_dE[x0] = valid ? sum : 0;
+    icm_dE[x1] = valid ? -sum : 0;
+  }
+  pc.lap(PHASE_ICM_APPLY);
+  // the last CTA to finish runs the exchange of the round (as k_plain_icm)
+  __shared__ int s_last;
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctl->icm_done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (tid == 0) ctl->icm_done = 0;
+  plain_exchange_body(J, ctl, icm_dE, icm_valid, base, dm);
+}
+
 // Energies after the Houdayer moves and the exchange decisions of round
 // ctl->i (the spin permutation follows in k_plain_perm); advances ctl->i.
 // `base` is shared memory for Ec, Er and Dm; dm receives Dm for k_plain_perm.
@@ -1574,9 +1843,52 @@ __global__ void __launch_bounds__(256) k_plain_perm(const PtJob* __restrict__ jp
 // The grid stride is a multiple of qps, so every thread keeps one quad k for
 // all its tasks and accumulates its fixed-point ΔE sums in registers; a CTA
 // combines its threads per slot and adds one 64-bit atomic per slot.
-template <bool SELF, uint32_t DEG>
-__global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ jp, const PlainCtl* __restrict__ ctl,
-                                                     uint32_t color, long long* acc) {
+// Closes round ctl->i - 1 after its last sweep launch, in the launch's last
+// CTA, when the round takes no measurement: adds the fixed-point sweep sums to
+// the energies and tracks the ground state (a new minimum's state included),
+// as k_plain_head would; a measured round is left to k_plain_head.  `base`:
+// shared memory for Ec and Er.
+__device__ void plain_close_round(const PtJob& J, PlainCtl* ctl, long long* acc, char* base) {
+  const uint32_t tid = threadIdx.x;
+  const uint32_t ip = ctl->i - 1;
+  const bool measured = ip >= J.meas_init && (sched(J.sample, ip, J.meas_init, J.num_sweeps) ||
+                                              sched(J.sample_states, ip, J.meas_init, J.num_sweeps));
+  if (!measured) {
+    Smem S{};
+    S.Ec = (double*)base;
+    S.Er = (double*)(base + al16((size_t)J.C * J.ntp * 8));
+    S.W = J.W;
+    const uint32_t CN = J.C * J.ntp;
+    for (uint32_t x = tid; x < CN; x += blockDim.x) {
+      // written by other CTAs' atomics: read through L2
+      const long long a = (long long)__ldcg((const unsigned long long*)acc + x);
+      const long long aq = (long long)__ldcg((const unsigned long long*)acc + CN + x);
+      S.Ec[x] = J.Ec[x] + (double)a * TAMC_FX_INV;
+      S.Er[x] = J.Er[x] + (double)(a + aq) * TAMC_FX_INV;
+      acc[x] = 0;
+      acc[CN + x] = 0;
+    }
+    __syncthreads();
+    if (ip >= J.meas_init) {
+      const GsSnap g = gs_track(J, S, ip);
+      uint32_t m_cur = ctl->m_cur, s_cur = ctl->s_cur;  // unchanged: no measurement this round
+      measure_rest(J, J.F, S, J.F.sus, J.F.iperm, ip, m_cur, s_cur, g, nullptr);
+    }
+    for (uint32_t x = tid; x < CN; x += blockDim.x) {
+      J.Ec[x] = S.Ec[x];
+      J.Er[x] = S.Er[x];
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (!measured) ctl->pending = 0;
+    ctl->sweep_done = 0;
+  }
+}
+
+template <bool SELF, uint32_t DEG, bool CLOSE>
+__global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
+                                                     long long* acc) {
   extern __shared__ uint4 smem_u4[];
   const PtJob& J = *jp;
   Fx4* red = reinterpret_cast<Fx4*>(smem_u4);                 // [blockDim.x]
@@ -1634,6 +1946,17 @@ __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ j
       if (sum) atomicAdd((unsigned long long*)&acc[pass * CN + x], (unsigned long long)sum);
     }
     __syncthreads();
+  }
+  if (CLOSE) {
+    __shared__ int s_last;
+    if (threadIdx.x == 0) {
+      __threadfence();
+      s_last = atomicAdd(&ctl->sweep_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    plain_close_round(J, ctl, acc, reinterpret_cast<char*>(b4 + J.qps));
   }
 }
 
@@ -1712,10 +2035,72 @@ static size_t plain_icm_smem(const PtJob& j, int stage) {
 }
 size_t plain_icm_bytes(const PtJob& j) { return plain_icm_smem(j, 0); }
 
+// Cluster form of the plain Houdayer kernel: CL CTAs per (pair, slot), chosen
+// as the largest of 4 or 2 that keeps every CTA of the launch resident at
+// once, for rows of 4 or 6 entries with at most 2 sites per thread and range.
+// Returns false (and launches nothing) where it does not apply.
+template <uint32_t CL, uint32_t DEG, uint32_t PS>
+static void launch_icm_cl(cudaStream_t st, uint32_t nclusters, size_t smem, const PtJob* d_job, PlainCtl* ctl,
+                          long long* icm_dE, uint32_t* icm_valid, unsigned long long* dm) {
+  auto k = k_plain_icm_cl<CL, DEG, PS>;
+  TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nclusters * CL);
+  cfg.blockDim = dim3(1024);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  TAMC_CUDA(cudaLaunchKernelEx(&cfg, k, d_job, ctl, icm_dE, icm_valid, dm));
+}
+
+template <uint32_t CL, uint32_t DEG>
+static void launch_icm_cl_ps(cudaStream_t st, uint32_t ps, uint32_t nclusters, size_t smem, const PtJob* d_job,
+                             PlainCtl* ctl, long long* icm_dE, uint32_t* icm_valid, unsigned long long* dm) {
+  if (ps == 1) launch_icm_cl<CL, DEG, 1>(st, nclusters, smem, d_job, ctl, icm_dE, icm_valid, dm);
+  else launch_icm_cl<CL, DEG, 2>(st, nclusters, smem, d_job, ctl, icm_dE, icm_valid, dm);
+}
+
+static bool plain_launch_icm_cluster(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl,
+                                     long long* icm_dE, uint32_t* icm_valid, size_t smem_limit, uint32_t num_sms,
+                                     unsigned long long* dm) {
+  if (const char* e = getenv("TAMC_PLAIN_CLUSTER"))
+    if (e[0] == '0') return false;
+  const uint32_t deg = j.F.udeg;
+  if (j.icm_uf || !j.F.col16 || (deg != 4 && deg != 6)) return false;
+  const uint32_t nclusters = (j.C / 2) * (j.nt - j.lo);
+  const uint32_t T = 1024;
+  for (uint32_t CL : {4u, 2u}) {
+    if (nclusters * CL > num_sms) continue;
+    const uint32_t span = (j.n + CL - 1) / CL;
+    const uint32_t ps = (span + T - 1) / T;
+    if (ps > 2) continue;  // more sites per thread spill at 64 registers
+    const uint32_t psr = ps <= 1 ? 1 : 2;
+    const size_t smem = std::max(carve_icm_cl(nullptr, nullptr, j.n, T, psr, deg, CL),
+                                 plain_head_smem(j.n, j.C, j.ntp));
+    if (smem > smem_limit) continue;
+    if (CL == 4) {
+      if (deg == 4) launch_icm_cl_ps<4, 4>(st, psr, nclusters, smem, d_job, ctl, icm_dE, icm_valid, dm);
+      else launch_icm_cl_ps<4, 6>(st, psr, nclusters, smem, d_job, ctl, icm_dE, icm_valid, dm);
+    } else {
+      if (deg == 4) launch_icm_cl_ps<2, 4>(st, psr, nclusters, smem, d_job, ctl, icm_dE, icm_valid, dm);
+      else launch_icm_cl_ps<2, 6>(st, psr, nclusters, smem, d_job, ctl, icm_dE, icm_valid, dm);
+    }
+    return true;
+  }
+  return false;
+}
+
 bool plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, long long* icm_dE,
-                      uint32_t* icm_valid, size_t smem_limit, unsigned long long* dm) {
+                      uint32_t* icm_valid, size_t smem_limit, uint32_t num_sms, unsigned long long* dm) {
   const uint32_t nact = j.nt - j.lo, grid = (j.C / 2) * nact;
   if (!j.icm || grid == 0) return false;
+  if (plain_launch_icm_cluster(st, j, d_job, ctl, icm_dE, icm_valid, smem_limit, num_sms, dm)) return true;
   // as much staging as fits: words and adjacency, words only, nothing
   int stage = j.F.col16 ? 3 : 2;
   if (plain_icm_smem(j, stage) > smem_limit) stage = 2;
@@ -1743,28 +2128,37 @@ void plain_launch_perm(cudaStream_t st, const PtJob& j, const PtJob* d_job, cons
   TAMC_CUDA(cudaGetLastError());
 }
 
-void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, uint32_t color,
-                        uint32_t ntask, long long* acc, uint32_t grid_cap) {
-  const uint32_t T = 256;
-  uint32_t grid = std::max(1u, std::min(grid_cap, (ntask + T - 1) / T));
-  // grid * T must be a multiple of qps (each thread keeps one quad)
-  const uint32_t g = j.qps / std::gcd(j.qps, T);
-  grid = std::max(g, (grid + g - 1) / g * g);
-  const size_t smem = (size_t)T * sizeof(Fx4) + (size_t)j.qps * 16;
+template <bool CLOSE>
+static void plain_launch_sweep_t(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl,
+                                 uint32_t color, uint32_t grid, uint32_t T, size_t smem, long long* acc) {
   auto go = [&](auto k) {
     TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<grid, T, smem, st>>>(d_job, ctl, color, acc);
   };
   const uint32_t deg = j.F.udeg == 4 || j.F.udeg == 6 ? j.F.udeg : 0;
   if (j.self_loops) {
-    if (deg == 4) go(k_plain_sweep<true, 4>);
-    else if (deg == 6) go(k_plain_sweep<true, 6>);
-    else go(k_plain_sweep<true, 0>);
+    if (deg == 4) go(k_plain_sweep<true, 4, CLOSE>);
+    else if (deg == 6) go(k_plain_sweep<true, 6, CLOSE>);
+    else go(k_plain_sweep<true, 0, CLOSE>);
   } else {
-    if (deg == 4) go(k_plain_sweep<false, 4>);
-    else if (deg == 6) go(k_plain_sweep<false, 6>);
-    else go(k_plain_sweep<false, 0>);
+    if (deg == 4) go(k_plain_sweep<false, 4, CLOSE>);
+    else if (deg == 6) go(k_plain_sweep<false, 6, CLOSE>);
+    else go(k_plain_sweep<false, 0, CLOSE>);
   }
+}
+
+void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, uint32_t color,
+                        uint32_t ntask, long long* acc, uint32_t grid_cap) {
+  const uint32_t T = 256;
+  uint32_t grid = std::max(1u, std::min(grid_cap, (ntask + T - 1) / T));
+  // grid * T must be a multiple of qps (each thread keeps one quad)
+  const uint32_t g = j.qps / std::gcd(j.qps, T);
+  grid = std::max(g, (grid + g - 1) / g * g);
+  const bool last = color + 1 == j.F.ncolors;
+  // the last colour's launch also closes the round: Ec and Er in shared memory
+  const size_t smem = (size_t)T * sizeof(Fx4) + (size_t)j.qps * 16 + (last ? 2 * al16((size_t)j.C * j.ntp * 8) : 0);
+  if (last) plain_launch_sweep_t<true>(st, j, d_job, ctl, color, grid, T, smem, acc);
+  else plain_launch_sweep_t<false>(st, j, d_job, ctl, color, grid, T, smem, acc);
   TAMC_CUDA(cudaGetLastError());
 }
 

@@ -53,6 +53,7 @@ struct PlainCtl {
   uint32_t s_cur;    // next state-snapshot index
   uint32_t pending;  // the sweeps of round i-1 ran; their sums and measurements are pending
   uint32_t icm_done; // Houdayer CTAs of the current round that finished (reset by the last)
+  uint32_t sweep_done; // CTAs of the round's last sweep launch that finished (reset by the last)
 };
 // with stage: room to hold the replica words and weights of a measured round
 size_t plain_head_bytes(const PtJob& j, bool stage);
@@ -60,18 +61,22 @@ size_t plain_head_bytes(const PtJob& j, bool stage);
 void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem,
                        int stage);
 size_t plain_icm_bytes(const PtJob& j);
-// Houdayer moves of round ctl->i, one CTA per (chain pair, slot >= lo); the
-// last CTA also runs the exchange decisions (writing dm).  Returns false, and
-// launches nothing, when the round has no Houdayer move.
+// Houdayer moves of round ctl->i, one CTA (or cluster) per (chain pair, slot
+// >= lo); the last CTA also runs the exchange decisions (writing dm).  Returns
+// false, and launches nothing, when the round has no Houdayer move.
+// With rows of 4 or 6 entries, each (pair, slot) runs on a cluster of 2 or 4
+// CTAs over distributed shared memory (TAMC_PLAIN_CLUSTER=0 keeps one CTA).
 bool plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, long long* icm_dE,
-                      uint32_t* icm_valid, size_t smem_limit, unsigned long long* dm);
+                      uint32_t* icm_valid, size_t smem_limit, uint32_t num_sms, unsigned long long* dm);
 // energies after ICM and the exchange decisions; advances ctl->i
 void plain_launch_exch(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, const long long* icm_dE,
                        uint32_t* icm_valid, unsigned long long* dm);
 // the exchange's spin permutation over all site words
 void plain_launch_perm(cudaStream_t st, const PtJob& j, const PtJob* d_job, const unsigned long long* dm,
                        uint32_t grid_cap);
-void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, const PlainCtl* ctl, uint32_t color,
+// one launch per colour class; the last class's launch also closes the round
+// when it takes no measurement (energies, ground-state tracking)
+void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, uint32_t color,
                         uint32_t ntask, long long* acc, uint32_t grid_cap);
 void plain_launch_init(cudaStream_t st, const PtJob* d_job, long long* acc, int random, uint32_t grid);
 

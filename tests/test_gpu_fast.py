@@ -413,3 +413,30 @@ def test_pt_fast_measurements_match_final_state(tb, po, gpu, monkeypatch, form, 
     last = np.unpackbits(words[-1].view(np.uint8), bitorder="little")[:n]
     s = (1 - 2 * last.astype(np.int8))[None]
     assert _rel_ok(np.array([en[-1]]), _f64_energies(po, text, s).reshape(1))
+
+
+@pytest.mark.parametrize("kind", ["3d_L8_64", "2d_L32_32", "3d_L16_64_c4"])
+def test_plain_cluster_houdayer_kernel_identical_to_one_cta(tb, po, gpu, monkeypatch, kind):
+    """The plain form's Houdayer move on 2- or 4-CTA clusters (sites split over
+    the CTAs, cluster words shared through distributed shared memory) runs the
+    same chain as the one-CTA kernel: states, energies, ground-state log,
+    samples, acceptance and round trips bit for bit."""
+    if kind == "3d_L8_64":
+        text, nt, C, sweeps = gi.lattice(8, 3, "gauss", 11), 64, 2, 40
+    elif kind == "2d_L32_32":
+        text, nt, C, sweeps = gi.lattice(32, 2, "pm", 12), 32, 4, 40
+    else:  # the C4 shape, a short run
+        text, nt, C, sweeps = gi.lattice(16, 3, "gauss", 0), 64, 2, 30
+    b = po.geometric_betas(0.2, 5.0, nt)
+    p = _pt(tb, sweeps, b, po.lo_beta_idx(b, lo_beta=1.0), C, 8, 5, 7, 0)
+    d = gpu.upload(tb.HostInstance.parse(text))
+    monkeypatch.setenv("TAMC_PT_FORM", "plain")
+    out = []
+    for cl in ("1", "0"):
+        monkeypatch.setenv("TAMC_PLAIN_CLUSTER", cl)
+        r = tb.PtRun(d, p, 77).run().sync()
+        ts = r.samples()
+        out.append([*r.state(), *r.gs(), np.array(ts.e), np.array(ts.q), np.array(ts.samples), r.acceptance(),
+                    *r.round_trips()])
+    for a, c in zip(out[0], out[1]):
+        assert np.array_equal(a, c)
