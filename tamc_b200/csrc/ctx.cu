@@ -236,6 +236,13 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
       for (size_t e = 0; e < fent.size(); ++e) c16[e] = (uint16_t)fent[e].x;
       d->d_fcol16 = dmalloc_copy(c16.data(), c16.size());
     }
+    // +-J instances (every coupling +-1, no field, no self-coupling, rows of 4 or
+    // 6 entries) take the multi-spin-coded sweep of the colour-ordered mode
+    d->pmj = (d->udeg == 4 || d->udeg == 6) && !d->self_loops;
+    for (uint32_t s = 0; s < h.n && d->pmj; ++s)
+      if (fbias[s] != 0.0f) d->pmj = 0;
+    for (size_t e = 0; e < fent.size() && d->pmj; ++e)
+      if ((fent[e].y & 0x7fffffffu) != 0x3f800000u) d->pmj = 0;  // |J| == 1.0f
     d->d_fbias = dmalloc_copy(fbias.data(), fbias.size());
     d->d_fkd = dmalloc_copy(fkd.data(), fkd.size());
     d->d_fsus = dmalloc_copy(fsus.data(), fsus.size());

@@ -85,6 +85,7 @@ enum : uint32_t {
   PTAG_INIT = 0x494eu,    // initial spins
   PTAG_ICM = 0x4943u,     // ICM seed-site choice
   PTAG_EXCH = 0x4558u,    // replica-exchange uniforms
+  PTAG_MSC = 0x4d53u,     // random words of the multi-spin-coded sweep
 };
 
 __host__ __device__ __forceinline__ uint2 philox_key(uint64_t seed) {
@@ -222,6 +223,7 @@ struct tamc_inst {
   uint2* d_fent = nullptr;           // nnz (col_new, J bits)
   uint16_t* d_fcol16 = nullptr;      // nnz col_new as 16 bits, padded to 8 entries (n <= 65536 only)
   uint32_t udeg = 0;                 // entries per row when every row has the same count, else 0
+  int pmj = 0;                       // +-1 couplings, no field, no self-loop, rows of 4 or 6 entries
   float* d_fbias = nullptr;          // n
   float* d_fkd = nullptr;            // n: self-loop coefficient (0 if none)
   double* d_fsus = nullptr;          // [nchi][n] colour order

@@ -22,6 +22,7 @@ struct FastInst {  // colour-ordered instance (device pointers)
   const uint2* ent;           // nnz (new column, J bits)
   const uint16_t* col16;      // nnz new column as 16 bits, padded to 8 entries; null if n > 65536
   uint32_t udeg;              // entries per row if uniform (row s = [s*udeg, (s+1)*udeg)), else 0
+  int pmj;                    // +-1 couplings, zero field, no self-loop, udeg 4 or 6 (multi-spin coding)
   const float* bias;          // n
   const float* kd;            // n self-loop coefficient
   const double* sus;          // [nchi][n], colour order
@@ -159,6 +160,126 @@ __device__ __forceinline__ float4 energy_terms4(uint32_t s, uint32_t shift, cons
 // (the same rule as rand_ising_state's Uniform(0,1), src/ising.rs:172).
 __device__ __forceinline__ uint32_t init_nibble(uint4 r) {
   return (r.x >> 31 ^ 1u) | ((r.y >> 31 ^ 1u) << 1) | ((r.z >> 31 ^ 1u) << 2) | ((r.w >> 31 ^ 1u) << 3);
+}
+
+// 32x32 bit transpose across a warp: lane L passes row L (bit c = column c)
+// and gets column L (bit r = row r's bit L).  Five butterfly steps; at step j
+// the lanes L and L^j swap the off-diagonal j x j blocks of their 2j x 2j tile.
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane) {
+  uint32_t m = 0x0000ffffu;
+#pragma unroll
+  for (uint32_t j = 16; j != 0; j >>= 1, m ^= m << j) {
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+    x = (lane & j) ? ((x & ~m) | ((y & ~m) >> j)) : ((x & m) | ((y & m) << j));
+  }
+  return x;
+}
+
+// ------------------------------------------------- multi-spin coding ----
+// For +-J instances (every J = +-1, no field, rows of DEG = 4 or 6 entries) a
+// site update acts on the 32 replicas of one word at once.  Bond (s, j) is
+// unsatisfied in replica r (it adds +1 to the energy) when J s_s s_j = +1;
+// with the bit convention (1 = spin -1) that is bit r of
+// ~(W_s ^ W_j ^ neg_J).  With x unsatisfied bonds the flip costs
+// dE = 2 (DEG - 2 x): x >= DEG / 2 always flips, x < DEG / 2 flips with
+// probability exp(-beta dE).  That probability, for the replica's beta and
+// level x, is held as a 32-bit threshold T = floor(p 2^32), stored bit-plane
+// by bit-plane (plane k: bit r = bit k of replica r's T); a uniform 32-bit
+// u < T decides, compared from the top bit down against random words, one
+// bit of u per word for all undecided replicas at once, so a word costs a few
+// random words instead of 32 uniforms.  u is uniform, so each replica flips
+// with probability T / 2^32 (within 2^-32 of p).
+//   planes: MscPlanes of the word (levels 0 .. DEG/2 - 1)
+struct MscLevels {
+  uint32_t lv[3];  // replicas at level x = 0, 1, 2 (x < DEG/2 only)
+  uint32_t p0, p1, p2;  // bit planes of x
+};
+
+template <uint32_t DEG>
+__device__ __forceinline__ MscLevels msc_levels(uint32_t S0, const uint32_t* Wj, uint32_t negmask) {
+  uint32_t p0 = 0, p1 = 0, p2 = 0;
+#pragma unroll
+  for (uint32_t m = 0; m < DEG; ++m) {
+    const uint32_t u = ~(S0 ^ Wj[m] ^ (0u - ((negmask >> m) & 1u)));
+    const uint32_t c0 = p0 & u;
+    p0 ^= u;
+    const uint32_t c1 = p1 & c0;
+    p1 ^= c0;
+    p2 ^= c1;
+  }
+  MscLevels L;
+  L.p0 = p0;
+  L.p1 = p1;
+  L.p2 = p2;
+  const uint32_t z = ~(p0 | p1 | p2);
+  L.lv[0] = z;                      // x = 0
+  L.lv[1] = p0 & ~p1 & ~p2;         // x = 1
+  L.lv[2] = DEG == 6 ? (~p0 & p1 & ~p2) : 0u;  // x = 2 (uphill only for DEG 6)
+  return L;
+}
+
+// The flip mask of one word: `pl` = threshold planes [DEG/2][32] of the word,
+// `al` / `nv` = replicas whose level always / never flips ([DEG/2]); random
+// words from Philox keyed by `key` and counted by (s, i, (wo << 8) | call).
+template <uint32_t DEG>
+__device__ __forceinline__ uint32_t msc_flip(const MscLevels& L, const uint32_t* pl, const uint32_t* al,
+                                             const uint32_t* nv, uint32_t s, uint32_t i, uint32_t wo, uint2 key) {
+  constexpr uint32_t LV = DEG / 2;
+  uint32_t uphill = 0, always = 0, und = 0;
+#pragma unroll
+  for (uint32_t l = 0; l < LV; ++l) {
+    uphill |= L.lv[l];
+    always |= L.lv[l] & al[l];
+    und |= L.lv[l] & ~al[l] & ~nv[l];
+  }
+  uint32_t lt = 0;
+  uint4 r = make_uint4(0, 0, 0, 0);
+  for (uint32_t k = 0; k < 32 && und; ++k) {
+    if ((k & 3u) == 0) r = philox4x32_10(make_uint4(s, i, (wo << 8) | (k >> 2), PTAG_MSC), key);
+    const uint32_t R = (k & 3u) == 0 ? r.x : (k & 3u) == 1 ? r.y : (k & 3u) == 2 ? r.z : r.w;
+    uint32_t t = 0;
+#pragma unroll
+    for (uint32_t l = 0; l < LV; ++l) t |= pl[l * 32 + (31 - k)] & L.lv[l];
+    lt |= und & ~R & t;
+    und &= ~(R ^ t);
+  }
+  return ~uphill | always | lt;
+}
+
+// Threshold planes of replica word `wo` for inverse temperatures beta[r]:
+// called by the 32 lanes of one warp, lane r for replica r of the word.
+template <uint32_t DEG>
+__device__ __forceinline__ void msc_planes(float beta, uint32_t lane, uint32_t* pl, uint32_t* al, uint32_t* nv) {
+  constexpr uint32_t LV = DEG / 2;
+#pragma unroll
+  for (uint32_t l = 0; l < LV; ++l) {
+    const double p = exp(-(double)beta * (double)(2 * ((int)DEG - 2 * (int)l)));
+    const bool a = !(p < 1.0);
+    const uint32_t T = a ? 0xffffffffu : (uint32_t)(p * 4294967296.0);
+    const uint32_t ab = __ballot_sync(0xffffffffu, a), zb = __ballot_sync(0xffffffffu, !a && T == 0);
+    for (uint32_t k = 0; k < 32; ++k) {
+      const uint32_t b = __ballot_sync(0xffffffffu, (T >> k) & 1u);
+      if (lane == 0) pl[l * 32 + k] = b;
+    }
+    if (lane == 0) {
+      al[l] = ab;
+      nv[l] = zb;
+    }
+  }
+}
+
+// Per-replica energy change of one word's flips, summed over the 32 lanes (32
+// sites of the same word): lane r receives the fixed-point sum for replica r.
+// dE = 2 (DEG - 2 x) per flip, so the sum is 2 DEG n_flip - 4 (n0 + 2 n1 + 4 n2)
+// with n_k the flips with bit k of x set.
+template <uint32_t DEG>
+__device__ __forceinline__ long long msc_energy(uint32_t flip, const MscLevels& L, uint32_t lane) {
+  const int nf = __popc(transpose32(flip, lane));
+  const int n0 = __popc(transpose32(flip & L.p0, lane));
+  const int n1 = __popc(transpose32(flip & L.p1, lane));
+  const int n2 = __popc(transpose32(flip & L.p2, lane));
+  const long long units = 2ll * DEG * nf - 4ll * (n0 + 2 * n1 + 4 * n2);
+  return units * 4294967296ll;  // to_fx of the integer energy change
 }
 
 }  // namespace tamc

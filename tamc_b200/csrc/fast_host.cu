@@ -178,6 +178,10 @@ static void fill_job(tamc_pt* pt, uint64_t seed, tamc_pt::FastState* F) {
   j.threaded = c.threads > 1;
   j.self_loops = I->self_loops;
   j.key = philox_key(seed);
+  // multi-spin-coded sweep for +-J instances (TAMC_MSC=0 keeps the per-quad update)
+  j.msc = j.F.pmj && (j.nw == 1 || j.nw == 2 || j.nw == 4);
+  if (const char* e = getenv("TAMC_MSC"))
+    if (e[0] == '0') j.msc = 0;
   cudaStream_t st = pt->g->stream;
   F->W.alloc((size_t)j.n * j.nw);
   F->Ec.alloc((size_t)j.C * j.ntp);

@@ -86,7 +86,11 @@ struct Smem {
   uint32_t* rp;
   float* bias;
   uint2* ent;
+  uint32_t* msc;  // multi-spin coding: per word [3][32] threshold planes, then [3] always, [3] never
 };
+
+// words of multi-spin-coding thresholds per replica word (levels x < 3)
+constexpr uint32_t MSC_WORDS = 3 * 32 + 3 + 3;
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
@@ -152,6 +156,7 @@ __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uin
   char* red = take((size_t)T * 16);
   char* redq = take((size_t)T * 16);
   char* Dm = take((size_t)C * 8);
+  char* msc = take((size_t)nw * MSC_WORDS * 4);
   char* rp = nullptr;
   char* bias = nullptr;
   char* ent = nullptr;
@@ -169,6 +174,7 @@ __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uin
     S->red = (float4*)red;
     S->redq = (float4*)redq;
     S->Dm = (unsigned long long*)Dm;
+    S->msc = (uint32_t*)msc;
     S->rp = (uint32_t*)rp;
     S->bias = (float*)bias;
     S->ent = (uint2*)ent;
@@ -1045,6 +1051,73 @@ __device__ void sweep_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t
   __syncthreads();
 }
 
+// Multi-spin-coded sweep of a +-J job (J.msc): warp w updates replica word
+// wo = w % nw of 32 consecutive sites of the colour class per step (lane =
+// site), the whole word at once (msc_flip); a lane owns its word, so no
+// atomics.  Per-replica energy changes are reduced over the warp's sites by
+// bit transposes and summed over warps in fixed point.  The threshold planes
+// of every word are in S.msc (msc_fill_planes).
+template <uint32_t DEG>
+__device__ __noinline__ void sweep_phase_msc(const PtJob& J, const FastInst& F, Smem& S, uint32_t i) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  const uint32_t nw = J.nw;
+  const uint32_t wo = warp % nw, step = nwarp / nw;
+  const uint32_t* pl = S.msc + wo * MSC_WORDS;
+  const uint32_t* al = pl + 96;
+  const uint32_t* nv = pl + 99;
+  long long e = 0;
+  for (uint32_t c = 0; c < F.ncolors; ++c) {
+    const uint32_t c0 = J.F.color_off[c], c1 = J.F.color_off[c + 1];
+    for (uint32_t base = c0 + (warp / nw) * 32u; base < c1; base += step * 32u) {
+      const uint32_t s = base + lane;
+      uint32_t flip = 0;
+      MscLevels L{};
+      if (s < c1) {
+        const uint32_t S0 = S.W[s * nw + wo];
+        uint32_t Wj[DEG], neg = 0;
+#pragma unroll
+        for (uint32_t m = 0; m < DEG; ++m) {
+          const uint2 ce = F.ent[s * DEG + m];
+          Wj[m] = S.W[ce.x * nw + wo];
+          neg |= (ce.y >> 31) << m;
+        }
+        L = msc_levels<DEG>(S0, Wj, neg);
+        flip = msc_flip<DEG>(L, pl, al, nv, s, i, wo, J.key);
+        S.W[s * nw + wo] = S0 ^ flip;
+      }
+      e += msc_energy<DEG>(flip, L, lane);
+    }
+    __syncthreads();
+  }
+  long long* red = reinterpret_cast<long long*>(S.red);  // nwarp * 32 entries (T * 8 of the 2 T * 16 bytes)
+  red[warp * 32 + lane] = e;
+  __syncthreads();
+  for (uint32_t x = tid; x < nw * 32; x += blockDim.x) {
+    const uint32_t w2 = x / 32, r = x % 32;
+    long long sum = 0;
+    for (uint32_t ww = w2; ww < nwarp; ww += nw) sum += red[ww * 32 + r];
+    const uint32_t c = w2 / J.wpc, t = (w2 % J.wpc) * 32 + r;
+    if (t < J.ntp) {
+      const uint32_t xx = c * J.ntp + t;
+      S.Ec[xx] += (double)sum * TAMC_FX_INV;
+      S.Er[xx] += (double)sum * TAMC_FX_INV;
+    }
+  }
+  __syncthreads();
+}
+
+// Threshold planes of every replica word of the job (warp w < nw fills word w).
+template <uint32_t DEG>
+__device__ __noinline__ void msc_fill_planes(const PtJob& J, uint32_t* msc) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  for (uint32_t wo = warp; wo < J.nw; wo += blockDim.x >> 5) {
+    const uint32_t t = (wo % J.wpc) * 32 + lane;
+    const float beta = t < J.ntp ? J.betas[t] : 0.0f;
+    uint32_t* pl = msc + wo * MSC_WORDS;
+    msc_planes<DEG>(beta, lane, pl, pl + 96, pl + 99);
+  }
+}
+
 __device__ __forceinline__ bool sched(int64_t period, uint32_t i, uint32_t meas_init, uint32_t num_sweeps) {
   return period >= 0 && i >= meas_init && ((i - meas_init) % (uint32_t)period == 0 || i == num_sweeps - 1);
 }
@@ -1093,19 +1166,6 @@ __device__ GsSnap gs_track(const PtJob& J, Smem& S, uint32_t i) {
   }
   __syncthreads();
   return s_g;
-}
-
-// 32x32 bit transpose across a warp: lane L passes row L (bit c = column c)
-// and gets column L (bit r = row r's bit L).  Five butterfly steps; at step j
-// the lanes L and L^j swap the off-diagonal j x j blocks of their 2j x 2j tile.
-__device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane) {
-  uint32_t m = 0x0000ffffu;
-#pragma unroll
-  for (uint32_t j = 16; j != 0; j >>= 1, m ^= m << j) {
-    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
-    x = (lane & j) ? ((x & ~m) | ((y & ~m) >> j)) : ((x & m) | ((y & m) << j));
-  }
-  return x;
 }
 
 // The rest of a round's measurements, after gs_track: the new minimum's
@@ -1271,6 +1331,10 @@ __device__ void run_job(const PtJob& J, char* smem_base) {
                              J.betas[4 * q + 3] * L2E);
   }
   const uint32_t Teff = (T / J.qps) * J.qps;
+  if (J.msc) {
+    if (F.udeg == 4) msc_fill_planes<4>(J, S.msc);
+    else msc_fill_planes<6>(J, S.msc);
+  }
   if (J.init == 1) {
     // random initial replicas, then their energies
     for (uint32_t x = tid; x < n * J.nw; x += T) {
@@ -1302,7 +1366,12 @@ __device__ void run_job(const PtJob& J, char* smem_base) {
     if (J.icm) icm_phase(J, F, S, i, pc);
     exchange_phase(J, S, i);
     pc.lap(PHASE_EXCH);
-    sweep_phase<SELF>(J, F, S, i, Teff);
+    if (J.msc) {
+      if (F.udeg == 4) sweep_phase_msc<4>(J, F, S, i);
+      else sweep_phase_msc<6>(J, F, S, i);
+    } else {
+      sweep_phase<SELF>(J, F, S, i, Teff);
+    }
     pc.lap(PHASE_SWEEP);
     if (i >= J.meas_init) measure_phase(J, F, S, i, m_cur, s_cur);
     pc.lap(PHASE_MEASURE);
@@ -1887,7 +1956,7 @@ __device__ void plain_close_round(const PtJob& J, PlainCtl* ctl, long long* acc,
 }
 
 template <bool SELF, uint32_t DEG, bool CLOSE>
-__global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
+__global__ void __launch_bounds__(256, 4) k_plain_sweep(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
                                                      long long* acc) {
   extern __shared__ uint4 smem_u4[];
   const PtJob& J = *jp;
@@ -1957,6 +2026,72 @@ __global__ void __launch_bounds__(256) k_plain_sweep(const PtJob* __restrict__ j
     if (!s_last) return;
     __threadfence();
     plain_close_round(J, ctl, acc, reinterpret_cast<char*>(b4 + J.qps));
+  }
+}
+
+// Multi-spin-coded sweep of one colour class for a +-J instance (J.msc): the
+// fused kernel's sweep_phase_msc spread over the grid -- global warp g updates
+// replica word g % nw of 32 consecutive sites per step -- with the same random
+// words, so both forms stay identical.  Per-replica energy sums: bit
+// transposes per warp, then one 64-bit atomic per replica and CTA.
+template <uint32_t DEG, bool CLOSE>
+__global__ void __launch_bounds__(256, 4) k_plain_sweep_msc(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
+                                                         long long* acc) {
+  extern __shared__ uint4 smem_u4[];
+  const PtJob& J = *jp;
+  const uint32_t nw = J.nw;
+  uint32_t* msc = reinterpret_cast<uint32_t*>(smem_u4);
+  long long* red = reinterpret_cast<long long*>(reinterpret_cast<char*>(smem_u4) + al16((size_t)nw * MSC_WORDS * 4));
+  msc_fill_planes<DEG>(J, msc);
+  __syncthreads();
+  const uint32_t i = ctl->i - 1;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const uint32_t gw = blockIdx.x * nwarp + warp, G = gridDim.x * nwarp;  // G % nw == 0
+  const uint32_t wo = gw % nw;
+  const uint32_t* pl = msc + wo * MSC_WORDS;
+  const uint32_t c0 = J.F.color_off[color], c1 = J.F.color_off[color + 1];
+  const uint2* __restrict__ ent = J.F.ent;
+  uint32_t* const W = J.W;
+  long long e = 0;
+  for (uint32_t base = c0 + (gw / nw) * 32u; base < c1; base += (G / nw) * 32u) {
+    const uint32_t s = base + lane;
+    uint32_t flip = 0;
+    MscLevels L{};
+    if (s < c1) {
+      const uint32_t S0 = W[s * nw + wo];
+      uint32_t Wj[DEG], neg = 0;
+#pragma unroll
+      for (uint32_t m = 0; m < DEG; ++m) {
+        const uint2 ce = ent[s * DEG + m];
+        Wj[m] = W[ce.x * nw + wo];
+        neg |= (ce.y >> 31) << m;
+      }
+      L = msc_levels<DEG>(S0, Wj, neg);
+      flip = msc_flip<DEG>(L, pl, pl + 96, pl + 99, s, i, wo, J.key);
+      W[s * nw + wo] = S0 ^ flip;
+    }
+    e += msc_energy<DEG>(flip, L, lane);
+  }
+  red[warp * 32 + lane] = e;
+  __syncthreads();
+  for (uint32_t x = threadIdx.x; x < nw * 32; x += blockDim.x) {
+    const uint32_t w2 = x / 32, r = x % 32;
+    long long sum = 0;
+    for (uint32_t ww = w2; ww < nwarp; ww += nw) sum += red[ww * 32 + r];  // warps of word w2 (nwarp % nw == 0)
+    const uint32_t c = w2 / J.wpc, t = (w2 % J.wpc) * 32 + r;
+    if (t < J.ntp && sum) atomicAdd((unsigned long long*)&acc[c * J.ntp + t], (unsigned long long)sum);
+  }
+  __syncthreads();
+  if (CLOSE) {
+    __shared__ int s_last;
+    if (threadIdx.x == 0) {
+      __threadfence();
+      s_last = atomicAdd(&ctl->sweep_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    plain_close_round(J, ctl, acc, reinterpret_cast<char*>(red + nwarp * 32));
   }
 }
 
@@ -2150,6 +2285,28 @@ static void plain_launch_sweep_t(cudaStream_t st, const PtJob& j, const PtJob* d
 void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, uint32_t color,
                         uint32_t ntask, long long* acc, uint32_t grid_cap) {
   const uint32_t T = 256;
+  if (j.msc) {
+    // one warp per (32 sites, word): ntask / qps sites in the class
+    const uint32_t nsites = ntask / j.qps;
+    const uint32_t warps = (nsites + 31) / 32 * j.nw;
+    const uint32_t grid = std::max(1u, std::min(grid_cap, (warps + T / 32 - 1) / (T / 32)));
+    const bool last = color + 1 == j.F.ncolors;
+    const size_t smem = al16((size_t)j.nw * MSC_WORDS * 4) + (size_t)(T / 32) * 32 * 8 +
+                        (last ? 2 * al16((size_t)j.C * j.ntp * 8) : 0);
+    auto go = [&](auto k) {
+      TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k<<<grid, T, smem, st>>>(d_job, ctl, color, acc);
+    };
+    if (j.F.udeg == 4) {
+      if (last) go(k_plain_sweep_msc<4, true>);
+      else go(k_plain_sweep_msc<4, false>);
+    } else {
+      if (last) go(k_plain_sweep_msc<6, true>);
+      else go(k_plain_sweep_msc<6, false>);
+    }
+    TAMC_CUDA(cudaGetLastError());
+    return;
+  }
   uint32_t grid = std::max(1u, std::min(grid_cap, (ntask + T - 1) / T));
   // grid * T must be a multiple of qps (each thread keeps one quad)
   const uint32_t g = j.qps / std::gcd(j.qps, T);

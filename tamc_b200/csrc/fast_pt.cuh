@@ -33,6 +33,8 @@ struct PtJob {
   uint32_t* count_out; // if set: receives the log count when the job's range is done
   unsigned long long* prof;  // if set: per-phase clock64 cycles (PHASE_* order), off otherwise
   uint64_t cost;       // sweeps * n * R, for longest-first ordering
+  int32_t msc;         // multi-spin-coded sweep (+-J instance, nw in {1, 2, 4})
+  int32_t pad_;
 };
 
 enum { PHASE_ICM_SCAN, PHASE_ICM_INIT, PHASE_ICM_JUMP, PHASE_ICM_GROW, PHASE_ICM_MARK, PHASE_ICM_APPLY, PHASE_EXCH,

@@ -36,6 +36,7 @@ FastInst make_fast_inst(const tamc_inst* d) {
   F.ent = d->d_fent;
   F.col16 = d->d_fcol16;
   F.udeg = d->udeg;
+  F.pmj = d->pmj;
   F.bias = d->d_fbias;
   F.kd = d->d_fkd;
   F.sus = d->d_fsus;
