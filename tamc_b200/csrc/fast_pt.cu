@@ -322,6 +322,54 @@ __device__ __forceinline__ void prop_passes(uint32_t n, uint32_t T, uint32_t tid
   }
 }
 
+// Energy change of flipping the clusters XC of the slots in gmask, for +-J
+// instances (rows of DEG entries, J = +-1, no field): a boundary bond (s in
+// the slot's cluster, j outside) that is unsatisfied in replica 0
+// (J s_s s_j = +1) changes by -2 when the cluster flips, a satisfied one by
+// +2.  Each lane takes a site; per slot bit, the counts of both kinds over the
+// site's bonds are bit-sliced (3 planes each), transposed across the warp
+// (lane b then holds slot b's counts over the warp's 32 sites) and added to
+// X.dE[b] (64-bit shared atomics; integer sums, so in any order); replica 1's
+// change is the negative.  X.dE must be zero on entry.
+template <uint32_t DEG, typename R0>
+__device__ __noinline__ void icm_energy_msc(uint32_t n, const uint32_t* XC, const uint2* __restrict__ ent, R0 r0,
+                                               uint32_t gmask, IcmScratch& X) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  long long acc = 0;
+  for (uint32_t base = warp * 32u; base < n; base += nwarp * 32u) {
+    const uint32_t s = base + lane;
+    uint32_t p0 = 0, p1 = 0, p2 = 0, q0 = 0, q1 = 0, q2 = 0;  // satisfied / unsatisfied boundary bonds
+    const uint32_t cs = s < n ? XC[s] : 0u;
+    if (cs) {
+      const uint32_t rs = r0(s);
+#pragma unroll
+      for (uint32_t m = 0; m < DEG; ++m) {
+        const uint2 ce = ent[s * DEG + m];
+        const uint32_t B = cs & ~XC[ce.x];
+        const uint32_t U = ~(rs ^ r0(ce.x) ^ (0u - (ce.y >> 31)));
+        const uint32_t a = B & ~U, b = B & U;
+        uint32_t c = p0 & a;
+        p0 ^= a;
+        p2 ^= p1 & c;
+        p1 ^= c;
+        c = q0 & b;
+        q0 ^= b;
+        q2 ^= q1 & c;
+        q1 ^= c;
+      }
+    }
+    const int dp = __popc(transpose32(p0, lane)) + 2 * __popc(transpose32(p1, lane)) +
+                   4 * __popc(transpose32(p2, lane));
+    const int dq = __popc(transpose32(q0, lane)) + 2 * __popc(transpose32(q1, lane)) +
+                   4 * __popc(transpose32(q2, lane));
+    acc += (long long)(2 * (dp - dq)) * 4294967296ll;
+  }
+  if (((gmask >> lane) & 1u) && acc) atomicAdd(&X.dE[lane], (unsigned long long)acc);
+  __syncthreads();
+  if (tid < 32 && ((gmask >> tid) & 1u)) X.dE[32 + tid] = (unsigned long long)(-(long long)X.dE[tid]);
+  __syncthreads();
+}
+
 template <bool PLAIN>
 __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScratch& X, uint32_t i, uint32_t p,
                           uint32_t w, uint32_t gmask, const uint16_t* cols = nullptr, uint32_t* wstage = nullptr,
@@ -712,6 +760,12 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
     if (pc) pc->lap(PHASE_ICM_GROW);
   }
   const uint32_t nlist = (uf || prop) ? n : X.q[3];
+  if (!PLAIN && F.pmj) {
+    // +-J instances: the boundary terms of every slot of the group at once,
+    // 32 sites per warp step (exact integers, so the same fixed-point sums)
+    if (F.udeg == 4) icm_energy_msc<4>(n, XC, ent, r0, gmask, X);
+    else icm_energy_msc<6>(n, XC, ent, r0, gmask, X);
+  } else
   // energy change of flipping each cluster in both replicas: boundary terms
   // -2 s_i (h_i + sum_{j not in cluster} J_ij s_j), f32 per site, summed in
   // fixed point per slot.  The slots are dealt to teams of warps (all warps
