@@ -111,12 +111,9 @@ struct Fx4 {
 // One quad update with inverse temperatures pre-scaled by 2 log2(e)
 // (TAMC_2LOG2E).  Returns the 4-bit flip mask; with ACC, adds accepted ΔE to
 // acc in fixed point.
-template <bool ACC, uint32_t DEG = 0>
-__device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
-                                                uint32_t ws, uint32_t wo, float4 b2, uint4 rnd, Fx4& acc) {
-  const float4 f = DEG ? local_field4_deg<DEG>(s, shift, F.ent, F.bias, W, ws, wo)
-                       : local_field4(s, shift, F.rp, F.ent, F.bias, W, ws, wo);
-  const uint32_t own = W[s * ws + wo] >> shift;
+// The decision of quad_update from the local field f and the quad's own spins.
+template <bool ACC>
+__device__ __forceinline__ uint32_t quad_accept(float4 f, uint32_t own, float4 b2, uint4 rnd, Fx4& acc) {
   const float4 g = spin_field4(f, own);
   const bool a0 = accept_g(g.x, b2.x, rnd.x);
   const bool a1 = accept_g(g.y, b2.y, rnd.y);
@@ -129,6 +126,20 @@ __device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, cons
     acc.w += to_fx(a3 ? -2.0f * g.w : 0.0f);
   }
   return (uint32_t)a0 | ((uint32_t)a1 << 1) | ((uint32_t)a2 << 2) | ((uint32_t)a3 << 3);
+}
+
+template <uint32_t DEG>
+__device__ __forceinline__ float4 quad_field(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
+                                             uint32_t ws, uint32_t wo) {
+  return DEG ? local_field4_deg<DEG>(s, shift, F.ent, F.bias, W, ws, wo)
+             : local_field4(s, shift, F.rp, F.ent, F.bias, W, ws, wo);
+}
+
+template <bool ACC, uint32_t DEG = 0>
+__device__ __forceinline__ uint32_t quad_update(uint32_t s, uint32_t shift, const FastInst& F, const uint32_t* W,
+                                                uint32_t ws, uint32_t wo, float4 b2, uint4 rnd, Fx4& acc) {
+  const float4 f = quad_field<DEG>(s, shift, F, W, ws, wo);
+  return quad_accept<ACC>(f, W[s * ws + wo] >> shift, b2, rnd, acc);
 }
 
 // Per-replica energy contribution of site s for a quad:

@@ -2010,7 +2010,7 @@ __device__ void plain_close_round(const PtJob& J, PlainCtl* ctl, long long* acc,
 }
 
 template <bool SELF, uint32_t DEG, bool CLOSE>
-__global__ void __launch_bounds__(256, 4) k_plain_sweep(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
+__global__ void __launch_bounds__(256, 3) k_plain_sweep(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
                                                      long long* acc) {
   extern __shared__ uint4 smem_u4[];
   const PtJob& J = *jp;
@@ -2037,19 +2037,40 @@ __global__ void __launch_bounds__(256, 4) k_plain_sweep(const PtJob* __restrict_
   const uint32_t nw = J.nw;
   const uint64_t s_first = gtid / J.qps, s_step = gstride / J.qps;
   Fx4 a{0, 0, 0, 0}, aq{0, 0, 0, 0};
-  for (uint64_t site = s_first; site < nc; site += s_step) {
-    const uint32_t s = c0 + (uint32_t)site;
-    const uint4 rnd = philox4x32_10(make_uint4(s, i, ch * 16u + q, PTAG_SWEEP), key);
-    const uint32_t m = quad_update<true, DEG>(s, shift, F, W, nw, wo, b2, rnd, a);
-    if (m) {
-      atomicXor(&W[s * nw + wo], m << shift);
-      if (SELF) {
-        const long long k2 = to_fx(2.0f * F.kd[s]);
-        aq.x += (m & 1u) ? k2 : 0;
-        aq.y += (m & 2u) ? k2 : 0;
-        aq.z += (m & 4u) ? k2 : 0;
-        aq.w += (m & 8u) ? k2 : 0;
-      }
+  // two sites of the class per step, all their loads issued before either is
+  // decided (sites of one colour class share no bond, so neither update can
+  // change what the other reads); the sums are integers, so the order of the
+  // updates does not matter
+  auto apply = [&](uint32_t s, uint32_t m) {
+    if (!m) return;
+    atomicXor(&W[s * nw + wo], m << shift);
+    if (SELF) {
+      const long long k2 = to_fx(2.0f * F.kd[s]);
+      aq.x += (m & 1u) ? k2 : 0;
+      aq.y += (m & 2u) ? k2 : 0;
+      aq.z += (m & 4u) ? k2 : 0;
+      aq.w += (m & 8u) ? k2 : 0;
+    }
+  };
+  for (uint64_t site = s_first; site < nc; site += 2 * s_step) {
+    const uint32_t sa = c0 + (uint32_t)site;
+    const bool two = site + s_step < nc;
+    const uint32_t sb = two ? c0 + (uint32_t)(site + s_step) : sa;
+    const float4 fa = quad_field<DEG>(sa, shift, F, W, nw, wo);
+    const uint32_t oa = W[sa * nw + wo] >> shift;
+    float4 fb = fa;
+    uint32_t ob = oa;
+    if (two) {
+      fb = quad_field<DEG>(sb, shift, F, W, nw, wo);
+      ob = W[sb * nw + wo] >> shift;
+    }
+    const uint32_t ma =
+        quad_accept<true>(fa, oa, b2, philox4x32_10(make_uint4(sa, i, ch * 16u + q, PTAG_SWEEP), key), a);
+    apply(sa, ma);
+    if (two) {
+      const uint32_t mb =
+          quad_accept<true>(fb, ob, b2, philox4x32_10(make_uint4(sb, i, ch * 16u + q, PTAG_SWEEP), key), a);
+      apply(sb, mb);
     }
   }
   const uint32_t CN = J.C * J.ntp;
