@@ -1,6 +1,8 @@
 // ctx.cu -- device contexts and device-resident instances.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "device.cuh"
 
@@ -59,6 +61,125 @@ static T* dmalloc_copy(const T* h, size_t count) {
   return d;
 }
 
+// The arrays of one instance upload, packed at 256-byte offsets into one host
+// staging buffer, then one device allocation and one copy.
+struct UploadPack {
+  std::vector<char> host;
+  std::vector<std::pair<void**, size_t>> slots;
+  template <class T>
+  void add(T** slot, const T* h, size_t count) {
+    const size_t off = (host.size() + 255) & ~(size_t)255;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    host.resize(off + bytes, 0);
+    if (count) memcpy(host.data() + off, h, count * sizeof(T));
+    slots.emplace_back(reinterpret_cast<void**>(slot), off);
+  }
+  void commit(void*& arena, size_t& bytes) {
+    bytes = host.size();
+    arena = dev_alloc(bytes);
+    TAMC_CUDA(copy_sync(arena, host.data(), bytes, cudaMemcpyHostToDevice));
+    for (auto& s : slots) *s.first = static_cast<char*>(arena) + s.second;
+  }
+};
+
+// ---------------------------------------------------- device-memory cache ----
+namespace {
+std::mutex g_cache_mu;
+struct DevCache {
+  std::map<size_t, std::vector<void*>> ready, pending;
+  size_t bytes = 0;
+};
+std::map<int, DevCache> g_cache;
+constexpr size_t kCacheMaxBlock = 8u << 20;      // larger blocks bypass the cache
+constexpr size_t kCacheMaxBytes = 1ull << 30;    // per device
+size_t size_class(size_t b) {
+  size_t c = 256;
+  while (c < b) c <<= 1;
+  return c;
+}
+void free_all_locked(DevCache& C) {
+  for (auto* m : {&C.ready, &C.pending})
+    for (auto& kv : *m)
+      for (void* p : kv.second) cudaFree(p);
+  C.ready.clear();
+  C.pending.clear();
+  C.bytes = 0;
+}
+}  // namespace
+
+void* dev_alloc(size_t bytes) {
+  bytes = std::max<size_t>(bytes, 1);
+  void* p = nullptr;
+  if (bytes > kCacheMaxBlock) {
+    if (cudaMalloc(&p, bytes) != cudaSuccess) fail(TAMC_E_NOMEM, "device allocation failed");
+    return p;
+  }
+  int dev = 0;
+  TAMC_CUDA(cudaGetDevice(&dev));
+  const size_t c = size_class(bytes);
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    DevCache& C = g_cache[dev];
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      auto it = C.ready.find(c);
+      if (it != C.ready.end() && !it->second.empty()) {
+        p = it->second.back();
+        it->second.pop_back();
+        C.bytes -= c;
+        return p;
+      }
+      if (attempt == 0 && !C.pending.empty()) {
+        // freed blocks become reusable once nothing in flight can still read them
+        TAMC_CUDA(cudaDeviceSynchronize());
+        for (auto& kv : C.pending) {
+          auto& r = C.ready[kv.first];
+          r.insert(r.end(), kv.second.begin(), kv.second.end());
+        }
+        C.pending.clear();
+      }
+    }
+  }
+  if (cudaMalloc(&p, c) != cudaSuccess) {
+    cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> lk(g_cache_mu);
+      cudaDeviceSynchronize();
+      free_all_locked(g_cache[dev]);
+    }
+    if (cudaMalloc(&p, c) != cudaSuccess) fail(TAMC_E_NOMEM, "device allocation failed");
+  }
+  return p;
+}
+
+void dev_free(void* p, size_t bytes) {
+  if (!p) return;
+  bytes = std::max<size_t>(bytes, 1);
+  if (bytes > kCacheMaxBlock) {
+    cudaFree(p);
+    return;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  const size_t c = size_class(bytes);
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  DevCache& C = g_cache[dev];
+  if (C.bytes + c > kCacheMaxBytes) {
+    cudaFree(p);
+    return;
+  }
+  C.pending[c].push_back(p);
+  C.bytes += c;
+}
+
+void dev_cache_release(int device) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto it = g_cache.find(device);
+  if (it == g_cache.end()) return;
+  cudaDeviceSynchronize();
+  free_all_locked(it->second);
+  g_cache.erase(it);
+}
+
 }  // namespace tamc
 
 using namespace tamc;
@@ -70,6 +191,7 @@ void tamc_gpu_release(tamc_gpu* g) {
   cudaStreamSynchronize(g->stream);
   cudaFree(g->d_exp);
   cudaStreamDestroy(g->stream);
+  dev_cache_release(g->device);
   delete g;
 }
 void tamc_inst_retain(tamc_inst* d) { d->refs.fetch_add(1); }
@@ -77,10 +199,7 @@ void tamc_inst_release(tamc_inst* d) {
   if (d->refs.fetch_sub(1) != 1) return;
   tamc_gpu* g = d->g;
   cudaSetDevice(g->device);
-  void* ptrs[] = {d->d_rp, d->d_col, d->d_J, d->d_bias, d->d_grp, d->d_gcol, d->d_sus, d->d_color_off,
-                  d->d_perm, d->d_iperm, d->d_frp, d->d_fent, d->d_fcol16, d->d_fbias, d->d_fkd, d->d_fsus};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  if (d->arena) dev_free(d->arena, d->arena_bytes);  // holds every array of the instance
   d->sa_scratch.release();
   delete d;
   tamc_gpu_release(g);
@@ -174,10 +293,11 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
   d->self_loops = h.has_self_loops();
   for (uint32_t i = 0; i < h.n; ++i) d->max_deg = std::max(d->max_deg, h.row_ptr[i + 1] - h.row_ptr[i]);
   try {
-    d->d_rp = dmalloc_copy(h.row_ptr.data(), h.row_ptr.size());
-    d->d_col = dmalloc_copy(h.col.data(), h.col.size());
-    d->d_J = dmalloc_copy(h.J.data(), h.J.size());
-    d->d_bias = dmalloc_copy(h.bias.data(), h.bias.size());
+    UploadPack pack;
+    pack.add(&d->d_rp, h.row_ptr.data(), h.row_ptr.size());
+    pack.add(&d->d_col, h.col.data(), h.col.size());
+    pack.add(&d->d_J, h.J.data(), h.J.size());
+    pack.add(&d->d_bias, h.bias.data(), h.bias.size());
     // ICM graph: off-diagonal entries over the petgraph node range
     d->g_nodes = h.graph_nodes();
     std::vector<uint32_t> grp(d->g_nodes + 1, 0), gcol;
@@ -186,11 +306,11 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
         if (h.col[e] != i) gcol.push_back(h.col[e]);
       grp[i + 1] = (uint32_t)gcol.size();
     }
-    d->d_grp = dmalloc_copy(grp.data(), grp.size());
-    d->d_gcol = dmalloc_copy(gcol.data(), gcol.size());
+    pack.add(&d->d_grp, grp.data(), grp.size());
+    pack.add(&d->d_gcol, gcol.data(), gcol.size());
     std::vector<double> sus((size_t)d->nchi * h.n);
     for (uint32_t k = 0; k < d->nchi; ++k) std::copy(h.suscept[k].begin(), h.suscept[k].end(), sus.begin() + (size_t)k * h.n);
-    d->d_sus = dmalloc_copy(sus.data(), sus.size());
+    pack.add(&d->d_sus, sus.data(), sus.size());
     // colour order
     std::vector<uint32_t> color;
     h.coloring(d->ncolors, color);
@@ -223,18 +343,18 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
       frp[s + 1] = (uint32_t)fent.size();
       for (uint32_t k = 0; k < d->nchi; ++k) fsus[(size_t)k * h.n + s] = h.suscept[k][i];
     }
-    d->d_color_off = dmalloc_copy(d->color_off.data(), d->color_off.size());
-    d->d_perm = dmalloc_copy(d->h_perm.data(), d->h_perm.size());
-    d->d_iperm = dmalloc_copy(iperm.data(), iperm.size());
-    d->d_frp = dmalloc_copy(frp.data(), frp.size());
+    pack.add(&d->d_color_off, d->color_off.data(), d->color_off.size());
+    pack.add(&d->d_perm, d->h_perm.data(), d->h_perm.size());
+    pack.add(&d->d_iperm, iperm.data(), iperm.size());
+    pack.add(&d->d_frp, frp.data(), frp.size());
     d->udeg = h.n ? frp[1] : 0;
     for (uint32_t s = 0; s < h.n && d->udeg; ++s)
       if (frp[s + 1] - frp[s] != d->udeg) d->udeg = 0;
-    d->d_fent = dmalloc_copy(fent.data(), fent.size());
+    pack.add(&d->d_fent, fent.data(), fent.size());
     if (h.n <= 65536) {
       std::vector<uint16_t> c16((fent.size() + 7) / 8 * 8 + 8, 0);
       for (size_t e = 0; e < fent.size(); ++e) c16[e] = (uint16_t)fent[e].x;
-      d->d_fcol16 = dmalloc_copy(c16.data(), c16.size());
+      pack.add(&d->d_fcol16, c16.data(), c16.size());
     }
     // +-J instances (every coupling +-1, no field, no self-coupling, rows of 4 or
     // 6 entries) take the multi-spin-coded sweep of the colour-ordered mode
@@ -243,9 +363,10 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
       if (fbias[s] != 0.0f) d->pmj = 0;
     for (size_t e = 0; e < fent.size() && d->pmj; ++e)
       if ((fent[e].y & 0x7fffffffu) != 0x3f800000u) d->pmj = 0;  // |J| == 1.0f
-    d->d_fbias = dmalloc_copy(fbias.data(), fbias.size());
-    d->d_fkd = dmalloc_copy(fkd.data(), fkd.size());
-    d->d_fsus = dmalloc_copy(fsus.data(), fsus.size());
+    pack.add(&d->d_fbias, fbias.data(), fbias.size());
+    pack.add(&d->d_fkd, fkd.data(), fkd.size());
+    pack.add(&d->d_fsus, fsus.data(), fsus.size());
+    pack.commit(d->arena, d->arena_bytes);
   } catch (...) {
     tamc_gpu_instance_destroy(d);
     throw;

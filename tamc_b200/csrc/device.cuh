@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "expf_exact.h"
@@ -36,6 +37,17 @@ inline cudaError_t copy_sync(void* dst, const void* src, size_t bytes, cudaMemcp
   count_copy(bytes, kind);
   return cudaMemcpy(dst, src, bytes, kind);
 }
+
+// Device memory of the library's handles (on the current device).  Blocks up
+// to a few MiB come from a per-device cache of freed blocks in power-of-two
+// size classes: a freed block first waits in a pending list and becomes
+// reusable only after one device synchronisation, so memory that work still
+// in flight on any stream reads is never handed out again.  Creating and
+// destroying many small runs then costs no cudaMalloc / cudaFree each.
+void* dev_alloc(size_t bytes);
+void dev_free(void* p, size_t bytes);
+// Returns the cached blocks of `device` to the driver.
+void dev_cache_release(int device);
 
 // ------------------------------------------------------------ RNG ----
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of the
@@ -165,10 +177,10 @@ struct SaScratch {
   void ensure(size_t nwords, size_t ne, size_t npacked, size_t nbetas) {
     auto grow = [](auto*& p, size_t& cap, size_t want, size_t elt) {
       if (want <= cap) return;
-      if (p) cudaFree(p);
+      if (p) tamc::dev_free(p, cap * elt);
       p = nullptr;
       cap = 0;
-      if (cudaMalloc((void**)&p, want * elt) != cudaSuccess) tamc::fail(TAMC_E_NOMEM, "device allocation failed");
+      p = static_cast<std::remove_reference_t<decltype(p)>>(tamc::dev_alloc(want * elt));
       cap = want;
     };
     grow(words, cap_words, nwords, 4);
@@ -177,10 +189,10 @@ struct SaScratch {
     grow(betas, cap_betas, nbetas, 4);
   }
   void release() {
-    if (words) cudaFree(words);
-    if (energies) cudaFree(energies);
-    if (packed) cudaFree(packed);
-    if (betas) cudaFree(betas);
+    if (words) tamc::dev_free(words, cap_words * 4);
+    if (energies) tamc::dev_free(energies, cap_e * 4);
+    if (packed) tamc::dev_free(packed, cap_packed);
+    if (betas) tamc::dev_free(betas, cap_betas * 4);
     words = nullptr;
     energies = nullptr;
     packed = nullptr;
@@ -225,6 +237,8 @@ struct tamc_inst {
   uint32_t udeg = 0;                 // entries per row when every row has the same count, else 0
   int pmj = 0;                       // +-1 couplings, no field, no self-loop, rows of 4 or 6 entries
   float* d_fbias = nullptr;          // n
+  void* arena = nullptr;             // one allocation holding every array above
+  size_t arena_bytes = 0;
   float* d_fkd = nullptr;            // n: self-loop coefficient (0 if none)
   double* d_fsus = nullptr;          // [nchi][n] colour order
   // host copies used by drivers

@@ -257,6 +257,50 @@ __device__ __forceinline__ uint32_t msc_flip(const MscLevels& L, const uint32_t*
   return ~uphill | always | lt;
 }
 
+// msc_flip for two words of the same site at once (words wo and wo + 1, each
+// with its own planes and random words): the same decisions, with the two
+// random streams interleaved so that their Philox rounds overlap.
+template <uint32_t DEG>
+__device__ __forceinline__ void msc_flip2(const MscLevels& L0, const MscLevels& L1, const uint32_t* pl0,
+                                          const uint32_t* pl1, uint32_t s, uint32_t i, uint32_t wo, uint2 key,
+                                          uint32_t& f0, uint32_t& f1) {
+  constexpr uint32_t LV = DEG / 2;
+  const uint32_t *al0 = pl0 + 96, *nv0 = pl0 + 99, *al1 = pl1 + 96, *nv1 = pl1 + 99;
+  uint32_t up0 = 0, alw0 = 0, und0 = 0, up1 = 0, alw1 = 0, und1 = 0;
+#pragma unroll
+  for (uint32_t l = 0; l < LV; ++l) {
+    up0 |= L0.lv[l];
+    alw0 |= L0.lv[l] & al0[l];
+    und0 |= L0.lv[l] & ~al0[l] & ~nv0[l];
+    up1 |= L1.lv[l];
+    alw1 |= L1.lv[l] & al1[l];
+    und1 |= L1.lv[l] & ~al1[l] & ~nv1[l];
+  }
+  uint32_t lt0 = 0, lt1 = 0;
+  uint4 r0 = make_uint4(0, 0, 0, 0), r1 = r0;
+  for (uint32_t k = 0; k < 32 && (und0 | und1); ++k) {
+    if ((k & 3u) == 0) {
+      if (und0) r0 = philox4x32_10(make_uint4(s, i, (wo << 8) | (k >> 2), PTAG_MSC), key);
+      if (und1) r1 = philox4x32_10(make_uint4(s, i, ((wo + 1) << 8) | (k >> 2), PTAG_MSC), key);
+    }
+    const uint32_t q = k & 3u;
+    const uint32_t R0 = q == 0 ? r0.x : q == 1 ? r0.y : q == 2 ? r0.z : r0.w;
+    const uint32_t R1 = q == 0 ? r1.x : q == 1 ? r1.y : q == 2 ? r1.z : r1.w;
+    uint32_t t0 = 0, t1 = 0;
+#pragma unroll
+    for (uint32_t l = 0; l < LV; ++l) {
+      t0 |= pl0[l * 32 + (31 - k)] & L0.lv[l];
+      t1 |= pl1[l * 32 + (31 - k)] & L1.lv[l];
+    }
+    lt0 |= und0 & ~R0 & t0;
+    und0 &= ~(R0 ^ t0);
+    lt1 |= und1 & ~R1 & t1;
+    und1 &= ~(R1 ^ t1);
+  }
+  f0 = ~up0 | alw0 | lt0;
+  f1 = ~up1 | alw1 | lt1;
+}
+
 // Threshold planes of replica word `wo` for inverse temperatures beta[r]:
 // called by the 32 lanes of one warp, lane r for replica r of the word.
 template <uint32_t DEG>

@@ -559,7 +559,11 @@ struct ChunkRunner {
   // whose rounds cost less than the costliest run's gets proportionally more
   // rounds (up to 8x), so that every run does about the same work per launch
   // and small runs are not held back by large ones (the serving loop).
-  void run(tamc_gpu* g, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance = false) {
+  // With `lazy_logs` the ground-state logs stay on the device until they could
+  // overflow in the next chunk (at most one entry per round) or are read
+  // (tamc_gpu_pt_gs drains them), instead of one readback per job and chunk.
+  void run(tamc_gpu* g, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance = false,
+           bool lazy_logs = false) {
     cudaStream_t st = g->stream;
     act.erase(std::remove_if(act.begin(), act.end(),
                              [](tamc_pt* p) { return p->next_sweep >= p->cfg.num_sweeps; }),
@@ -662,8 +666,9 @@ struct ChunkRunner {
       pt->m_next += count_sched(c.sample, c.meas_init, c.num_sweeps, pt->next_sweep, ends[x]);
       pt->s_next += count_sched(c.sample_states, c.meas_init, c.num_sweeps, pt->next_sweep, ends[x]);
       pt->next_sweep = ends[x];
-      if (h_counts[x]) pt->out.drain(st);
-      else pt->out.pending = 0;
+      const uint32_t next = std::min(pt->out.cap, balance ? 8 * chunk : chunk);
+      if (h_counts[x] && (!lazy_logs || h_counts[x] + next > pt->out.cap)) pt->out.drain(st);
+      else if (!h_counts[x]) pt->out.pending = 0;
     }
   }
 };
@@ -720,7 +725,7 @@ int tamc_gpu_batch_run(tamc_batch* b) {
     bool any = false;
     for (auto* pt : b->jobs) any |= pt->next_sweep < pt->cfg.num_sweeps;
     if (!any) break;
-    b->runner.run(b->g, b->jobs, b->chunk, true);
+    b->runner.run(b->g, b->jobs, b->chunk, true, false, true);
   }
   TAMC_API_END
 }

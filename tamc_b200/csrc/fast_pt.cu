@@ -1115,41 +1115,54 @@ template <uint32_t DEG>
 __device__ __noinline__ void sweep_phase_msc(const PtJob& J, const FastInst& F, Smem& S, uint32_t i) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
   const uint32_t nw = J.nw;
-  const uint32_t wo = warp % nw, step = nwarp / nw;
+  // words in pairs (wo, wo + 1) per lane when nw is even: two independent
+  // random streams in flight per lane; nw == 1 takes the single-word path
+  const uint32_t per = nw == 1 ? 1u : 2u, ng = nw / per;
+  const uint32_t g = warp % ng, step = nwarp / ng;
+  const uint32_t wo = g * per;
   const uint32_t* pl = S.msc + wo * MSC_WORDS;
-  const uint32_t* al = pl + 96;
-  const uint32_t* nv = pl + 99;
-  long long e = 0;
+  long long e0 = 0, e1 = 0;
   for (uint32_t c = 0; c < F.ncolors; ++c) {
     const uint32_t c0 = J.F.color_off[c], c1 = J.F.color_off[c + 1];
-    for (uint32_t base = c0 + (warp / nw) * 32u; base < c1; base += step * 32u) {
+    for (uint32_t base = c0 + (warp / ng) * 32u; base < c1; base += step * 32u) {
       const uint32_t s = base + lane;
-      uint32_t flip = 0;
-      MscLevels L{};
+      uint32_t f0 = 0, f1 = 0;
+      MscLevels L0{}, L1{};
       if (s < c1) {
+        uint32_t Wj0[DEG], Wj1[DEG], neg = 0;
         const uint32_t S0 = S.W[s * nw + wo];
-        uint32_t Wj[DEG], neg = 0;
+        const uint32_t S1 = per == 2 ? S.W[s * nw + wo + 1] : 0u;
 #pragma unroll
         for (uint32_t m = 0; m < DEG; ++m) {
           const uint2 ce = F.ent[s * DEG + m];
-          Wj[m] = S.W[ce.x * nw + wo];
+          Wj0[m] = S.W[ce.x * nw + wo];
+          Wj1[m] = per == 2 ? S.W[ce.x * nw + wo + 1] : 0u;
           neg |= (ce.y >> 31) << m;
         }
-        L = msc_levels<DEG>(S0, Wj, neg);
-        flip = msc_flip<DEG>(L, pl, al, nv, s, i, wo, J.key);
-        S.W[s * nw + wo] = S0 ^ flip;
+        L0 = msc_levels<DEG>(S0, Wj0, neg);
+        if (per == 2) {
+          L1 = msc_levels<DEG>(S1, Wj1, neg);
+          msc_flip2<DEG>(L0, L1, pl, pl + MSC_WORDS, s, i, wo, J.key, f0, f1);
+          S.W[s * nw + wo + 1] = S1 ^ f1;
+        } else {
+          f0 = msc_flip<DEG>(L0, pl, pl + 96, pl + 99, s, i, wo, J.key);
+        }
+        S.W[s * nw + wo] = S0 ^ f0;
       }
-      e += msc_energy<DEG>(flip, L, lane);
+      e0 += msc_energy<DEG>(f0, L0, lane);
+      if (per == 2) e1 += msc_energy<DEG>(f1, L1, lane);
     }
     __syncthreads();
   }
-  long long* red = reinterpret_cast<long long*>(S.red);  // nwarp * 32 entries (T * 8 of the 2 T * 16 bytes)
-  red[warp * 32 + lane] = e;
+  long long* red = reinterpret_cast<long long*>(S.red);  // nwarp * 64 entries (the 2 T * 16 bytes of red, redq)
+  red[(warp * 2) * 32 + lane] = e0;
+  red[(warp * 2 + 1) * 32 + lane] = e1;
   __syncthreads();
   for (uint32_t x = tid; x < nw * 32; x += blockDim.x) {
     const uint32_t w2 = x / 32, r = x % 32;
+    const uint32_t gg = w2 / per, k = w2 % per;  // word w2 is member k of pair gg
     long long sum = 0;
-    for (uint32_t ww = w2; ww < nwarp; ww += nw) sum += red[ww * 32 + r];
+    for (uint32_t ww = gg; ww < nwarp; ww += ng) sum += red[(ww * 2 + k) * 32 + r];
     const uint32_t c = w2 / J.wpc, t = (w2 % J.wpc) * 32 + r;
     if (t < J.ntp) {
       const uint32_t xx = c * J.ntp + t;

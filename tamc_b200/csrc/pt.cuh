@@ -15,14 +15,14 @@ struct DBuf {  // owning device buffer
   DBuf() = default;
   explicit DBuf(size_t count) { alloc(count); }
   void alloc(size_t count) {
-    if (p) cudaFree(p);
+    if (p) dev_free(p, std::max<size_t>(n, 1) * sizeof(T));
     p = nullptr;
     n = count;
-    TAMC_CUDA(cudaMalloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T)));
+    p = static_cast<T*>(dev_alloc(std::max<size_t>(count, 1) * sizeof(T)));
   }
   void zero(cudaStream_t st) { TAMC_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), st)); }
   ~DBuf() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p, std::max<size_t>(n, 1) * sizeof(T));
   }
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;

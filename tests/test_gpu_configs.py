@@ -11,12 +11,9 @@
 * C4 shortened (3-D L=16 Gaussian, 64 temperatures, 1000 sweeps, 8 seeds):
   <E> over the paramagnetic temperatures against the oracle.
 
-Statistical rule (fixed before any run): z = (mean_gpu - mean_oracle) /
-sqrt(se_gpu^2 + se_oracle^2) over independent seeds; every |z| <= 4 and at
-least 95 % of them <= 3.  With 128 comparisons (C1) a strict "all within 3
-standard errors" would fail by chance about one run in three (expected 0.35
-exceedances at p = 0.0027 each), so the 3-sigma bound is applied to the bulk
-and a 4-sigma bound to every quantity.
+Statistical rule (tests/stat_rule.py, fixed before any run): z = (mean_gpu -
+mean_oracle) / sqrt(se_gpu^2 + se_oracle^2) over independent seeds; every
+|z| <= 4 and at least 95 % of them <= 3.
 """
 import concurrent.futures as cf
 import math
@@ -33,15 +30,8 @@ CORES = os.cpu_count() or 1
 
 
 def _z_ok(g, o, label):
-    """g, o: [seeds][k] per-seed means; applies the module's statistical rule."""
-    g, o = np.asarray(g, np.float64), np.asarray(o, np.float64)
-    se = np.sqrt(g.var(0, ddof=1) / len(g) + o.var(0, ddof=1) / len(o))
-    d = g.mean(0) - o.mean(0)
-    both_fixed = se == 0
-    assert np.all(np.abs(d[both_fixed]) <= 1e-6 * np.maximum(1.0, np.abs(o.mean(0)[both_fixed]))), label
-    z = np.abs(d[~both_fixed]) / se[~both_fixed]
-    assert z.size == 0 or (z.max() <= 4.0 and np.mean(z <= 3.0) >= 0.95), (label, np.round(z, 2))
-    return z
+    from stat_rule import z_ok
+    return z_ok(g, o, label)
 
 
 def _thermal_stats(e, q, sus, nt, chains=2):
