@@ -194,6 +194,40 @@ def test_threaded_run_independent_of_omp_threads(po):
     assert np.array_equal(outs[0], outs[1])
 
 
+def test_oracle_serial_exchange_samples_exact_boltzmann_and_threaded_does_not(po):
+    """<E>(beta) of a 4x4 +-J torus against exact enumeration of its 65536
+    states.  Serial exchange (threads: 1, tamc-core/src/pt.rs:120-132)
+    updates the next pair's energy difference after a swap: every |z| <= 4 over
+    6 runs.  The threaded exchange (tamc-core/src/parallel/pt.rs:46-58) decides
+    every pair on the differences of the round's start; the oracle keeps that,
+    and its coldest slot is visibly hotter than the Boltzmann average."""
+    from tamc_b200 import instances as gi
+    text = gi.lattice(4, 2, "pm", 21)
+    betas = np.linspace(0.1, 1.6, 8).astype(np.float32)
+    spins = ((np.arange(1 << 16)[:, None] >> np.arange(16)[None, :]) & 1).astype(np.int8) * -2 + 1
+    E = np.zeros(1 << 16)
+    for ln in text.strip().splitlines():
+        a, c, k = ln.split()
+        E += float(k) * spins[:, int(a)] * spins[:, int(c)]
+    exact = np.array([(np.exp(-float(b) * (E - E.min())) * E).sum() / np.exp(-float(b) * (E - E.min())).sum()
+                      for b in betas])
+    inst = po.Instance.from_text(text)
+
+    def means(threads):
+        out = []
+        for s in range(6):
+            r = po.PtRun(inst, betas, 20000, 0.1, 4, True, 2, threads, sample=1, seed=900 + s)
+            r.run(nthreads=1)
+            out.append(np.array(r.thermal()[0], np.float64).mean(axis=1))
+        out = np.array(out)
+        return out.mean(0), out.std(0, ddof=1) / np.sqrt(len(out))
+
+    m1, se1 = means(1)
+    assert np.all(np.abs(m1 - exact) <= 4 * se1), (m1, exact, se1)
+    m4, se4 = means(4)
+    assert m4[-1] - exact[-1] > 0.2 and m4[-1] - exact[-1] > 20 * se4[-1], (m4, exact)
+
+
 @pytest.mark.parametrize("threads", [1, 3])
 def test_oracle_qubo_cached_energy_rule(po, threads):
     """The oracle's cached energies on a QUBO follow the reference's rule
