@@ -520,8 +520,11 @@ struct ChunkRunner {
   uint32_t cap_jobs = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  uint32_t g_n = 0, g_grid = 0, g_T = 0;
-  size_t g_smem = 0;
+  uint32_t g_key[8] = {};  // launch shape of the captured graph
+  // second stream and fork/join events of the two-class launch
+  cudaStream_t aux = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  int prio_hi = 0, prio_lo = 0;
   // device time of the chunk launches (CUDA events around each one: the job
   // table upload, the fused kernel and the count readback) and their number
   cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -531,6 +534,9 @@ struct ChunkRunner {
     reset();
     for (auto e : ev)
       if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (aux) cudaStreamDestroy(aux);
   }
   void reset() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -552,9 +558,45 @@ struct ChunkRunner {
     TAMC_CUDA(cudaMallocHost((void**)&h_jobs, cap_jobs * sizeof(PtJob)));
     TAMC_CUDA(cudaMallocHost((void**)&h_counts, cap_jobs * sizeof(uint32_t)));
     d_jobs.alloc(cap_jobs);
-    ctr.alloc(1);
+    ctr.alloc(2);
     counts.alloc(cap_jobs);
   }
+  // The CTA size, shared memory and grid of one persistent launch over `grp`:
+  // T0 raised to 512 where a run's quads need it, halved while the largest
+  // run's shared memory does not fit (TAMC_PT_CSR=0 keeps every CSR in HBM).
+  struct Launch {
+    uint32_t T = 0, grid = 0;
+    size_t smem = 0;
+    int per_sm = 0;
+  };
+  static Launch shape(tamc_gpu* g, std::vector<tamc_pt*>& grp, uint32_t T) {
+    const char* csr_env = getenv("TAMC_PT_CSR");
+    uint32_t qps_max = 0;
+    for (auto* pt : grp) {
+      if (T < pt->fast->job.qps) T = 512;
+      qps_max = std::max(qps_max, pt->fast->job.qps);
+    }
+    size_t smem = 0;
+    for (;;) {  // the largest run decides: smaller CTAs leave more shared memory
+      smem = 0;
+      for (auto* pt : grp) {
+        PtJob& j = pt->fast->job;
+        if (csr_env && csr_env[0] == '0') j.csr_smem = 0;
+        if (fused_smem_bytes(j, T, j.csr_smem) > g->smem_optin) j.csr_smem = 0;
+        smem = std::max(smem, fused_smem_bytes(j, T, j.csr_smem));
+      }
+      if (smem <= g->smem_optin || T / 2 < std::max(128u, qps_max)) break;
+      T /= 2;
+    }
+    if (smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "a run is too large for the fused PT kernel");
+    Launch L;
+    L.T = T;
+    L.smem = smem;
+    L.per_sm = fused_blocks_per_sm(T, smem);
+    L.grid = std::min<uint32_t>((uint32_t)grp.size(), (uint32_t)(g->num_sms * std::max(L.per_sm, 1)));
+    return L;
+  }
+
   // Advances every run in `act` by up to `chunk` rounds.  With `balance`, a run
   // whose rounds cost less than the costliest run's gets proportionally more
   // rounds (up to 8x), so that every run does about the same work per launch
@@ -562,6 +604,12 @@ struct ChunkRunner {
   // With `lazy_logs` the ground-state logs stay on the device until they could
   // overflow in the next chunk (at most one entry per round) or are read
   // (tamc_gpu_pt_gs drains them), instead of one readback per job and chunk.
+  // Runs autotuned to 512 threads and runs autotuned to fewer go to two
+  // persistent launches that share the GPU (two streams, forked and joined by
+  // events, in one graph): the large runs' launch at the higher launch
+  // priority, one CTA per SM, and the small runs' launch beside it with two or
+  // more CTAs per SM, so that small runs no longer hold a whole SM each after
+  // the large ones have taken theirs (TAMC_PT_SPLIT=0: one launch).
   void run(tamc_gpu* g, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance = false,
            bool lazy_logs = false) {
     cudaStream_t st = g->stream;
@@ -573,31 +621,46 @@ struct ChunkRunner {
       return (uint64_t)(p->cfg.num_sweeps - p->next_sweep) * (p->fast->job.cost / std::max(1u, p->cfg.num_sweeps));
     };
     std::stable_sort(act.begin(), act.end(), [&](tamc_pt* x, tamc_pt* y) { return remaining(x) > remaining(y); });
-    // one CTA size per launch: the autotuned size of the costliest run
-    // (TAMC_PT_T and TAMC_PT_CSR=0 override it for measurements)
-    uint32_t T = act[0]->fast->T;
-    if (const char* e = getenv("TAMC_PT_T")) {
-      const int t = atoi(e);
-      if (t == 128 || t == 256 || t == 512) T = (uint32_t)t;
-    }
-    const char* csr_env = getenv("TAMC_PT_CSR");
-    for (auto* pt : act)
-      if (T < pt->fast->job.qps) T = 512;
-    uint32_t qps_max = 0;
-    for (auto* pt : act) qps_max = std::max(qps_max, pt->fast->job.qps);
-    size_t smem = 0;
-    for (;;) {  // the largest run decides: smaller CTAs leave more shared memory
-      smem = 0;
+    const char* t_env = getenv("TAMC_PT_T");
+    const char* split_env = getenv("TAMC_PT_SPLIT");
+    Launch A, B;
+    bool split = false;
+    uint32_t nb = (uint32_t)act.size();
+    if (!t_env && !(split_env && split_env[0] == '0')) {
+      std::vector<tamc_pt*> big, small;
+      uint32_t Ts = 128;
       for (auto* pt : act) {
-        PtJob& j = pt->fast->job;
-        if (csr_env && csr_env[0] == '0') j.csr_smem = 0;
-        if (fused_smem_bytes(j, T, j.csr_smem) > g->smem_optin) j.csr_smem = 0;
-        smem = std::max(smem, fused_smem_bytes(j, T, j.csr_smem));
+        if (pt->fast->T >= 512) big.push_back(pt);
+        else {
+          small.push_back(pt);
+          Ts = std::max(Ts, pt->fast->T);
+        }
       }
-      if (smem <= g->smem_optin || T / 2 < std::max(128u, qps_max)) break;
-      T /= 2;
+      if (const char* e = getenv("TAMC_PT_TSMALL")) {  // the small class's CTA size, for measurements
+        const int t = atoi(e);
+        if (t == 128 || t == 256) Ts = (uint32_t)t;
+      }
+      if (!big.empty() && !small.empty()) {
+        A = shape(g, big, 512);
+        B = shape(g, small, Ts);
+        split = B.per_sm >= 2 && B.T < A.T;
+        if (split) {
+          nb = (uint32_t)big.size();
+          act = big;
+          act.insert(act.end(), small.begin(), small.end());
+        }
+      }
     }
-    if (smem > g->smem_optin) fail(TAMC_E_UNSUPPORTED, "a run is too large for the fused PT kernel");
+    if (!split) {
+      // one CTA size per launch: the autotuned size of the costliest run
+      // (TAMC_PT_T overrides it for measurements)
+      uint32_t T = act[0]->fast->T;
+      if (t_env) {
+        const int t = atoi(t_env);
+        if (t == 128 || t == 256 || t == 512) T = (uint32_t)t;
+      }
+      A = shape(g, act, T);
+    }
     const uint32_t na = (uint32_t)act.size();
     reserve(na);
     std::vector<uint32_t> ends(na);
@@ -620,10 +683,32 @@ struct ChunkRunner {
       j.count_out = counts.p + x;
       h_jobs[x] = j;
     }
-    const int per_sm = fused_blocks_per_sm(T, smem);
-    const uint32_t grid = std::min<uint32_t>(na, (uint32_t)(g->num_sms * std::max(per_sm, 1)));
+    if (split && !aux) {
+      int least = 0, greatest = 0;
+      TAMC_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      prio_hi = greatest;
+      prio_lo = least;
+      TAMC_CUDA(cudaStreamCreateWithPriority(&aux, cudaStreamNonBlocking, least));
+      TAMC_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+      TAMC_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    }
+    // the kernel launches of one chunk (both classes, or one launch)
+    auto launch_all = [&]() {
+      if (!split) {
+        fused_launch(st, d_jobs.p, na, ctr.p, A.grid, A.T, A.smem);
+        return;
+      }
+      fused_smem_limit(std::max(A.smem, B.smem));
+      TAMC_CUDA(cudaEventRecord(fork, st));
+      TAMC_CUDA(cudaStreamWaitEvent(aux, fork, 0));
+      fused_launch_prio(st, d_jobs.p, nb, ctr.p, A.grid, A.T, A.smem, prio_hi);
+      fused_launch_prio(aux, d_jobs.p + nb, na - nb, ctr.p + 1, B.grid, B.T, B.smem, prio_lo);
+      TAMC_CUDA(cudaEventRecord(join, aux));
+      TAMC_CUDA(cudaStreamWaitEvent(st, join, 0));
+    };
     if (use_graph) {
-      if (!exec || g_n != na || g_grid != grid || g_T != T || g_smem != smem) {
+      const uint32_t key[8] = {na, nb, A.grid, A.T, (uint32_t)A.smem, B.grid, B.T, (uint32_t)B.smem};
+      if (!exec || memcmp(key, g_key, sizeof(key)) != 0) {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr;
@@ -631,15 +716,12 @@ struct ChunkRunner {
         TAMC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         // the graph's two copies are counted at every replay below
         cudaMemcpyAsync(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st);
-        cudaMemsetAsync(ctr.p, 0, 4, st);
-        fused_launch(st, d_jobs.p, na, ctr.p, grid, T, smem);
+        cudaMemsetAsync(ctr.p, 0, 8, st);
+        launch_all();
         cudaMemcpyAsync(h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st);
         TAMC_CUDA(cudaStreamEndCapture(st, &graph));
         TAMC_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        g_n = na;
-        g_grid = grid;
-        g_T = T;
-        g_smem = smem;
+        memcpy(g_key, key, sizeof(key));
       }
       TAMC_CUDA(cudaEventRecord(ev[0], st));
       TAMC_CUDA(cudaGraphLaunch(exec, st));
@@ -649,12 +731,12 @@ struct ChunkRunner {
     } else {
       TAMC_CUDA(cudaEventRecord(ev[0], st));
       TAMC_CUDA(tamc::copy_async(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st));
-      TAMC_CUDA(cudaMemsetAsync(ctr.p, 0, 4, st));
-      fused_launch(st, d_jobs.p, na, ctr.p, grid, T, smem);
+      TAMC_CUDA(cudaMemsetAsync(ctr.p, 0, 8, st));
+      launch_all();
       TAMC_CUDA(tamc::copy_async(h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st));
       TAMC_CUDA(cudaEventRecord(ev[1], st));
     }
-    g->count();
+    g->count(split ? 2 : 1);
     TAMC_CUDA(cudaStreamSynchronize(st));
     float ms = 0.0f;
     TAMC_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));

@@ -27,6 +27,8 @@
 #include "fast_pt.cuh"
 
 #include <cooperative_groups.h>
+#include <map>
+#include <mutex>
 #include <numeric>
 
 namespace cg = cooperative_groups;
@@ -87,7 +89,53 @@ struct Smem {
   float* bias;
   uint2* ent;
   uint32_t* msc;  // multi-spin coding: per word [3][32] threshold planes, then [3] always, [3] never
+  // fused kernel: the exchange bookkeeping and the ground-state log's running
+  // minimum in shared memory for a range of rounds (XchgSm below); null in the
+  // plain form, which uses the job's global arrays
+  char* xb;
 };
+
+// Shared-memory copies of a fused job's exchange bookkeeping and of its
+// ground-state minimum, loaded at the start of a range of rounds and stored at
+// its end (no global round trips inside a round).  One base pointer: the
+// fields are found by offsets, which keeps the kernel's register budget.
+struct GsMin {
+  int have;
+  float minE;
+  uint32_t count;
+};
+struct XchgSm {
+  uint8_t* tags;    // [C][nt]
+  uint32_t* acc;    // [C][nt]
+  uint32_t* dhist;  // [C][nt][2]
+  uint32_t* rtrips; // [C]
+  float* dbeta;     // [nt - 1] beta[j + 1] - beta[j] (f32)
+  GsMin* gs;
+};
+__host__ __device__ inline size_t xchg_layout(XchgSm* X, char* base, uint32_t C, uint32_t nt) {
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    char* p = base ? base + o : nullptr;
+    o = (o + bytes + 15) & ~(size_t)15;
+    return p;
+  };
+  const size_t CT = (size_t)C * nt;
+  char* tags = take(CT);
+  char* acc = take(CT * 4);
+  char* dhist = take(CT * 8);
+  char* rtrips = take((size_t)C * 4);
+  char* dbeta = take((size_t)nt * 4);
+  char* gs = take(sizeof(GsMin));
+  if (X) {
+    X->tags = (uint8_t*)tags;
+    X->acc = (uint32_t*)acc;
+    X->dhist = (uint32_t*)dhist;
+    X->rtrips = (uint32_t*)rtrips;
+    X->dbeta = (float*)dbeta;
+    X->gs = (GsMin*)gs;
+  }
+  return o;
+}
 
 // words of multi-spin-coding thresholds per replica word (levels x < 3)
 constexpr uint32_t MSC_WORDS = 3 * 32 + 3 + 3;
@@ -157,6 +205,7 @@ __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uin
   char* redq = take((size_t)T * 16);
   char* Dm = take((size_t)C * 8);
   char* msc = take((size_t)nw * MSC_WORDS * 4);
+  char* xb = take(xchg_layout(nullptr, nullptr, C, ntp));
   char* rp = nullptr;
   char* bias = nullptr;
   char* ent = nullptr;
@@ -175,6 +224,7 @@ __host__ __device__ inline size_t carve_all(Smem* S, char* base, uint32_t n, uin
     S->redq = (float4*)redq;
     S->Dm = (unsigned long long*)Dm;
     S->msc = (uint32_t*)msc;
+    S->xb = xb;
     S->rp = (uint32_t*)rp;
     S->bias = (float*)bias;
     S->ent = (uint2*)ent;
@@ -917,6 +967,8 @@ __device__ void icm_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i
 __device__ void exchange_decide(const PtJob& J, Smem& S, uint32_t i) {
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const uint32_t nt = J.nt;
+  XchgSm XS{J.tags, J.acc, J.dhist, J.rtrips, nullptr, nullptr};
+  if (S.xb) xchg_layout(&XS, S.xb, J.C, J.ntp);
   for (uint32_t c = warp; c < J.C; c += nwarp) {
     double* Ec = S.Ec + c * J.ntp;
     double* Er = S.Er + c * J.ntp;
@@ -927,7 +979,7 @@ __device__ void exchange_decide(const PtJob& J, Smem& S, uint32_t i) {
         const uint32_t j = lane + 32u * h;
         if (j + 1 < nt) {
           const float des = (float)Ec[j + 1] - (float)Ec[j];
-          const float dlt = (J.betas[j + 1] - J.betas[j]) * des;
+          const float dlt = (S.xb ? XS.dbeta[j] : J.betas[j + 1] - J.betas[j]) * des;
           d[h] = dlt >= 0.0f ||
                  u24(philox4x32_10(make_uint4(j, i, c, PTAG_EXCH), J.key).x) < __expf(dlt);
         }
@@ -940,7 +992,7 @@ __device__ void exchange_decide(const PtJob& J, Smem& S, uint32_t i) {
         for (uint32_t j = 0; j + 1 < nt; ++j) {
           float des = (float)Ec[j + 1] - (float)Ec[j];
           if (prev) des += carry;  // ΔE propagation after a swap (tamc-core/src/pt.rs:138-141)
-          const float dlt = (J.betas[j + 1] - J.betas[j]) * des;
+          const float dlt = (S.xb ? XS.dbeta[j] : J.betas[j + 1] - J.betas[j]) * des;
           const bool dj = dlt >= 0.0f ||
                           u24(philox4x32_10(make_uint4(j, i, c, PTAG_EXCH), J.key).x) < __expf(dlt);
           if (dj) D |= 1ull << j;
@@ -951,8 +1003,8 @@ __device__ void exchange_decide(const PtJob& J, Smem& S, uint32_t i) {
       D = __shfl_sync(0xffffffffu, D, 0);
     }
     // acceptance counts, slot permutation of energies and tags, round trips
-    uint32_t* acc = J.acc + (size_t)c * nt;
-    uint8_t* tg = J.tags + (size_t)c * nt;
+    uint32_t* acc = XS.acc + (size_t)c * nt;
+    uint8_t* tg = XS.tags + (size_t)c * nt;
     double e_new[2], r_new[2];
     uint8_t t_new[2];
     for (int h = 0; h < 2; ++h) {
@@ -981,20 +1033,20 @@ __device__ void exchange_decide(const PtJob& J, Smem& S, uint32_t i) {
     if (lane == 0) {  // PTState::update_round_trips (tamc-core/src/pt.rs:54-72)
       uint8_t lo = tg[0];
       if (lo == 0) lo = 1;
-      else if (lo == 4) { J.rtrips[c] += 1; lo = 1; }
+      else if (lo == 4) { XS.rtrips[c] += 1; lo = 1; }
       else if (lo == 2) lo = 3;
       tg[0] = lo;
       uint8_t hi = tg[nt - 1];
       if (hi == 0) hi = 2;
-      else if (hi == 3) { J.rtrips[c] += 1; hi = 2; }
+      else if (hi == 3) { XS.rtrips[c] += 1; hi = 2; }
       else if (hi == 1) hi = 4;
       tg[nt - 1] = hi;
     }
     __syncwarp();
     for (uint32_t k = lane; k < nt; k += 32) {
       const uint8_t v = tg[k];
-      if (v == 1 || v == 3) J.dhist[((size_t)c * nt + k) * 2] += 1;
-      else if (v == 2 || v == 4) J.dhist[((size_t)c * nt + k) * 2 + 1] += 1;
+      if (v == 1 || v == 3) XS.dhist[((size_t)c * nt + k) * 2] += 1;
+      else if (v == 2 || v == 4) XS.dhist[((size_t)c * nt + k) * 2 + 1] += 1;
     }
     if (lane == 0) S.Dm[c] = D;
   }
@@ -1217,16 +1269,21 @@ __device__ GsSnap gs_track(const PtJob& J, Smem& S, uint32_t i) {
     }
     if (lane == 0) {
       GsSnap g{0, 0, 0, 0};
-      if (!*J.log.have || be < *J.log.minE) {
-        *J.log.have = 1;
-        *J.log.minE = be;
-        const uint32_t k = *J.log.count;
+      XchgSm XS{};
+      if (S.xb) xchg_layout(&XS, S.xb, J.C, J.ntp);
+      int* have = S.xb ? &XS.gs->have : J.log.have;
+      float* minE = S.xb ? &XS.gs->minE : J.log.minE;
+      uint32_t* count = S.xb ? &XS.gs->count : J.log.count;
+      if (!*have || be < *minE) {
+        *have = 1;
+        *minE = be;
+        const uint32_t k = *count;
         if (k < J.log.cap) {
           J.log.steps[k] = i;
           J.log.E[k] = be;
           g = GsSnap{1, k, bx / nt, bx % nt};
         }
-        *J.log.count = k + 1;
+        *count = k + 1;
       }
       s_g = g;
     }
@@ -1375,6 +1432,47 @@ __device__ __forceinline__ void load_job(PtJob& dst, const PtJob* src) {
   __syncthreads();
 }
 
+// The fused job's bookkeeping into shared memory (start of a range of rounds)
+// and back (its end); the end also reports the log count.
+__device__ __noinline__ void xchg_load(const PtJob& J, char* xb) {
+  XchgSm X;
+  xchg_layout(&X, xb, J.C, J.ntp);
+  const uint32_t CT = J.C * J.nt;
+  for (uint32_t x = threadIdx.x; x < CT; x += blockDim.x) {
+    X.tags[x] = J.tags[x];
+    X.acc[x] = J.acc[x];
+    X.dhist[2 * x] = J.dhist[2 * x];
+    X.dhist[2 * x + 1] = J.dhist[2 * x + 1];
+  }
+  for (uint32_t c = threadIdx.x; c < J.C; c += blockDim.x) X.rtrips[c] = J.rtrips[c];
+  for (uint32_t j = threadIdx.x; j + 1 < J.nt; j += blockDim.x) X.dbeta[j] = J.betas[j + 1] - J.betas[j];
+  if (threadIdx.x == 0) {
+    X.gs->have = *J.log.have;
+    X.gs->minE = *J.log.minE;
+    X.gs->count = *J.log.count;
+  }
+  __syncthreads();
+}
+__device__ __noinline__ void xchg_store(const PtJob& J, char* xb) {
+  XchgSm X;
+  xchg_layout(&X, xb, J.C, J.ntp);
+  const uint32_t CT = J.C * J.nt;
+  for (uint32_t x = threadIdx.x; x < CT; x += blockDim.x) {
+    J.tags[x] = X.tags[x];
+    J.acc[x] = X.acc[x];
+    J.dhist[2 * x] = X.dhist[2 * x];
+    J.dhist[2 * x + 1] = X.dhist[2 * x + 1];
+  }
+  for (uint32_t c = threadIdx.x; c < J.C; c += blockDim.x) J.rtrips[c] = X.rtrips[c];
+  if (threadIdx.x == 0) {
+    *J.log.have = X.gs->have;
+    *J.log.minE = X.gs->minE;
+    *J.log.count = X.gs->count;
+    if (J.count_out) *J.count_out = X.gs->count;
+  }
+  __syncthreads();
+}
+
 template <bool SELF>
 __device__ void run_job(const PtJob& J, char* smem_base) {
   Smem S;
@@ -1426,6 +1524,9 @@ __device__ void run_job(const PtJob& J, char* smem_base) {
     __syncthreads();
     if (J.init == 2) full_energies(J, F, S, Teff);
   }
+  // exchange bookkeeping and the ground-state minimum stay in shared memory
+  // for the range of rounds (no global round trips inside a round)
+  xchg_load(J, S.xb);
   uint32_t m_cur = J.m_base, s_cur = J.s_base;
   PhaseClock pc;
   pc.start(J.prof);
@@ -1448,8 +1549,7 @@ __device__ void run_job(const PtJob& J, char* smem_base) {
     J.Ec[x] = S.Ec[x];
     J.Er[x] = S.Er[x];
   }
-  if (tid == 0 && J.count_out) *J.count_out = *J.log.count;
-  __syncthreads();
+  xchg_store(J, S.xb);
 }
 
 __global__ void __launch_bounds__(512, 1) k_pt_fused(const PtJob* __restrict__ jobs, uint32_t njobs, uint32_t* ctr) {
@@ -2226,8 +2326,23 @@ size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem) {
   return carve_all(nullptr, nullptr, j.n, j.nw, j.C, j.ntp, j.qps, T, j.F.nnz, csr_smem, j.icm_group, j.icm_uf != 0);
 }
 
+// The fused kernel's dynamic shared-memory limit only grows (per device), so
+// that a captured launch stays valid whatever smaller launches ran since.
+static void fused_attr(size_t smem) {
+  static std::mutex mu;
+  static std::map<int, size_t> set;
+  int dev = 0;
+  TAMC_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = set[dev];
+  if (smem > cur) {
+    TAMC_CUDA(cudaFuncSetAttribute(k_pt_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cur = smem;
+  }
+}
+
 int fused_blocks_per_sm(uint32_t T, size_t smem) {
-  TAMC_CUDA(cudaFuncSetAttribute(k_pt_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fused_attr(smem);
   int nb = 0;
   TAMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_pt_fused, (int)T, smem));
   return nb;
@@ -2418,9 +2533,26 @@ void plain_launch_init(cudaStream_t st, const PtJob* d_job, long long* acc, int 
 
 void fused_launch(cudaStream_t st, const PtJob* d_jobs, uint32_t njobs, uint32_t* ctr, uint32_t grid, uint32_t T,
                   size_t smem) {
-  TAMC_CUDA(cudaFuncSetAttribute(k_pt_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fused_attr(smem);
   k_pt_fused<<<grid, T, smem, st>>>(d_jobs, njobs, ctr);
   TAMC_CUDA(cudaGetLastError());
 }
+
+void fused_launch_prio(cudaStream_t st, const PtJob* d_jobs, uint32_t njobs, uint32_t* ctr, uint32_t grid, uint32_t T,
+                       size_t smem, int priority) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributePriority;
+  at[0].val.priority = priority;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  TAMC_CUDA(cudaLaunchKernelEx(&cfg, k_pt_fused, d_jobs, njobs, ctr));
+}
+
+void fused_smem_limit(size_t smem) { fused_attr(smem); }
 
 }  // namespace tamc

@@ -47,6 +47,12 @@ int fused_blocks_per_sm(uint32_t T, size_t smem);
 // Launch over `njobs` jobs already on the device; `ctr` is a zeroed counter.
 void fused_launch(cudaStream_t st, const PtJob* d_jobs, uint32_t njobs, uint32_t* ctr, uint32_t grid,
                   uint32_t T, size_t smem);
+// A fused launch with a launch priority (cudaLaunchAttributePriority; lower
+// numbers run first); the shared-memory attribute must already cover `smem`
+// (fused_smem_limit).
+void fused_launch_prio(cudaStream_t st, const PtJob* d_jobs, uint32_t njobs, uint32_t* ctr, uint32_t grid, uint32_t T,
+                       size_t smem, int priority);
+void fused_smem_limit(size_t smem);
 
 // Plain form (one instance over the whole GPU, one launch per sweep phase).
 struct PlainCtl {

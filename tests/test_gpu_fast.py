@@ -278,6 +278,38 @@ def test_batch_equals_single_runs(tb, po, gpu):
         assert np.array_equal(r.acceptance(), batch.acceptance(k))
 
 
+def test_batch_two_class_launch_identical_to_one_launch(tb, po, gpu, monkeypatch):
+    """A batch that mixes runs autotuned to 512 threads (2-D L=32) with runs
+    autotuned to fewer (L=8, 12) goes to two concurrent persistent launches,
+    two or more small CTAs per SM; every result is the one of a single launch
+    (TAMC_PT_SPLIT=0) bit for bit."""
+    shapes = [(32, 32), (8, 16), (12, 24), (32, 16), (8, 32), (12, 16), (8, 24)]
+    runs = []
+    for split in ("1", "0"):
+        monkeypatch.setenv("TAMC_PT_SPLIT", split)
+        batch = tb.Batch(gpu)
+        for k, (L, nt) in enumerate(shapes):
+            b = po.geometric_betas(0.2, 5.0, nt)
+            d = gpu.upload(tb.HostInstance.parse(gi.lattice(L, 2, "pm", 300 + k)))
+            batch.add(d, tb.PtParams(80, b, po.lo_beta_idx(b, lo_beta=1.0), 0.5, True, 2, 8, 4, 8, 0), 70 + k)
+        n0 = gpu.launches
+        batch.run()
+        runs.append((batch, gpu.launches - n0))
+    (b1, l1), (b0, l0) = runs
+    tiles = {b1.tile(k)[0] for k in range(len(shapes))}
+    if 512 in tiles and min(tiles) < 512:
+        assert l1 == 2 * l0, (l1, l0, tiles)  # two kernel launches per chunk
+    for k in range(len(shapes)):
+        S1, E1 = b1.state(k)
+        S0, E0 = b0.state(k)
+        assert np.array_equal(S1, S0) and np.array_equal(E1, E0), k
+        assert np.array_equal(b1.gs(k)[1], b0.gs(k)[1])
+        assert np.array_equal(b1.acceptance(k), b0.acceptance(k))
+        assert np.array_equal(np.array(b1.samples(k).e), np.array(b0.samples(k).e))
+        t1, t0 = b1.round_trips(k), b0.round_trips(k)
+        assert all(np.array_equal(np.asarray(x), np.asarray(y)) for x, y in zip(t1, t0))
+
+
 def test_server_results_same_alone_and_in_the_mix(tb, po, gpu):
     jobs = _mixed_jobs(po, 7, 1)
     srv = tb.Server(gpu, hbm_budget_bytes=1 << 30, max_active=3, chunk_sweeps=40)
