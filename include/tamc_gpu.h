@@ -185,7 +185,9 @@ int tamc_gpu_pt_samples(tamc_pt* pt, float* e, int32_t* q, float* suscept, uint8
  * spent per round phase (ICM: seed scan, union-find label init, pointer
  * jumping, cluster growth (BFS levels or union-find hooking), cluster marking,
  * energy change and flip; exchange, sweep, measurement, other), summed over
- * rounds; zeros otherwise.  cycles[10]. */
+ * rounds, then four parts of the multi-spin-coded sweep of +-J instances summed
+ * over the CTA's warps (loads and bond levels, flip decisions, energy sums and
+ * stores, barrier waits); zeros otherwise.  cycles[14]. */
 int tamc_gpu_pt_phase_cycles(tamc_pt* pt, uint64_t* cycles);
 /* Wall time of the sweep loop in microseconds (the reference's `timing`). */
 double tamc_gpu_pt_timing_us(tamc_pt* pt);

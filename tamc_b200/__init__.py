@@ -473,7 +473,7 @@ class PtRun:
         return lib().tamc_gpu_pt_timing_us(self.h)
 
     PHASES = ("icm_scan", "icm_init", "icm_jump", "icm_grow", "icm_mark", "icm_apply", "exchange", "sweep", "measure",
-              "other")
+              "other", "sweep_levels_per_warp", "sweep_flip_per_warp", "sweep_energy_per_warp", "sweep_wait_per_warp")
 
     def phase_cycles(self) -> dict:
         """Cycles per round phase (fast mode, TAMC_PHASE_PROF=1 at creation)."""

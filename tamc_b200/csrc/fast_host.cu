@@ -627,15 +627,13 @@ struct ChunkRunner {
     bool split = false;
     uint32_t nb = (uint32_t)act.size();
     if (!t_env && !(split_env && split_env[0] == '0')) {
+      // the small class runs at 128 threads (four CTAs per SM by registers):
+      // on C3 that measured 27.6 ms per 1000 sweeps against 35.0 ms at the
+      // small runs' own autotuned 256 threads (two per SM), which time one
+      // run alone on an otherwise idle SM
       std::vector<tamc_pt*> big, small;
       uint32_t Ts = 128;
-      for (auto* pt : act) {
-        if (pt->fast->T >= 512) big.push_back(pt);
-        else {
-          small.push_back(pt);
-          Ts = std::max(Ts, pt->fast->T);
-        }
-      }
+      for (auto* pt : act) (pt->fast->T >= 512 ? big : small).push_back(pt);
       if (const char* e = getenv("TAMC_PT_TSMALL")) {  // the small class's CTA size, for measurements
         const int t = atoi(e);
         if (t == 128 || t == 256) Ts = (uint32_t)t;

@@ -1173,6 +1173,16 @@ __device__ __noinline__ void sweep_phase_msc(const PtJob& J, const FastInst& F, 
   const uint32_t g = warp % ng, step = nwarp / ng;
   const uint32_t wo = g * per;
   const uint32_t* pl = S.msc + wo * MSC_WORDS;
+  // sub-phase cycles per warp (lane 0) when profiling
+  unsigned long long* const prof = J.prof;
+  long long tl = (prof && lane == 0) ? clock64() : 0;
+  auto stamp = [&](int ph) {
+    if (prof && lane == 0) {
+      const long long t = clock64();
+      atomicAdd(&prof[ph], (unsigned long long)(t - tl));
+      tl = t;
+    }
+  };
   long long e0 = 0, e1 = 0;
   for (uint32_t c = 0; c < F.ncolors; ++c) {
     const uint32_t c0 = J.F.color_off[c], c1 = J.F.color_off[c + 1];
@@ -1180,10 +1190,11 @@ __device__ __noinline__ void sweep_phase_msc(const PtJob& J, const FastInst& F, 
       const uint32_t s = base + lane;
       uint32_t f0 = 0, f1 = 0;
       MscLevels L0{}, L1{};
+      uint32_t S0 = 0, S1 = 0;
       if (s < c1) {
         uint32_t Wj0[DEG], Wj1[DEG], neg = 0;
-        const uint32_t S0 = S.W[s * nw + wo];
-        const uint32_t S1 = per == 2 ? S.W[s * nw + wo + 1] : 0u;
+        S0 = S.W[s * nw + wo];
+        S1 = per == 2 ? S.W[s * nw + wo + 1] : 0u;
 #pragma unroll
         for (uint32_t m = 0; m < DEG; ++m) {
           const uint2 ce = F.ent[s * DEG + m];
@@ -1192,19 +1203,26 @@ __device__ __noinline__ void sweep_phase_msc(const PtJob& J, const FastInst& F, 
           neg |= (ce.y >> 31) << m;
         }
         L0 = msc_levels<DEG>(S0, Wj0, neg);
-        if (per == 2) {
-          L1 = msc_levels<DEG>(S1, Wj1, neg);
-          msc_flip2<DEG>(L0, L1, pl, pl + MSC_WORDS, s, i, wo, J.key, f0, f1);
-          S.W[s * nw + wo + 1] = S1 ^ f1;
-        } else {
-          f0 = msc_flip<DEG>(L0, pl, pl + 96, pl + 99, s, i, wo, J.key);
-        }
+        if (per == 2) L1 = msc_levels<DEG>(S1, Wj1, neg);
+      }
+      if (prof) __syncwarp();
+      stamp(PHASE_SW_LEVELS);
+      if (s < c1) {
+        if (per == 2) msc_flip2<DEG>(L0, L1, pl, pl + MSC_WORDS, s, i, wo, J.key, f0, f1);
+        else f0 = msc_flip<DEG>(L0, pl, pl + 96, pl + 99, s, i, wo, J.key);
+      }
+      if (prof) __syncwarp();
+      stamp(PHASE_SW_FLIP);
+      if (s < c1) {
+        if (per == 2) S.W[s * nw + wo + 1] = S1 ^ f1;
         S.W[s * nw + wo] = S0 ^ f0;
       }
       e0 += msc_energy<DEG>(f0, L0, lane);
       if (per == 2) e1 += msc_energy<DEG>(f1, L1, lane);
+      stamp(PHASE_SW_ENERGY);
     }
     __syncthreads();
+    stamp(PHASE_SW_WAIT);
   }
   long long* red = reinterpret_cast<long long*>(S.red);  // nwarp * 64 entries (the 2 T * 16 bytes of red, redq)
   red[(warp * 2) * 32 + lane] = e0;

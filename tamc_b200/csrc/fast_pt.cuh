@@ -38,7 +38,10 @@ struct PtJob {
 };
 
 enum { PHASE_ICM_SCAN, PHASE_ICM_INIT, PHASE_ICM_JUMP, PHASE_ICM_GROW, PHASE_ICM_MARK, PHASE_ICM_APPLY, PHASE_EXCH,
-       PHASE_SWEEP, PHASE_MEASURE, PHASE_OTHER, PHASE_N };
+       PHASE_SWEEP, PHASE_MEASURE, PHASE_OTHER,
+       // multi-spin-coded sweep, per warp (summed over warps): loads and bond
+       // levels, flip decisions, energy sums and stores, barrier waits
+       PHASE_SW_LEVELS, PHASE_SW_FLIP, PHASE_SW_ENERGY, PHASE_SW_WAIT, PHASE_N };
 
 // Shared-memory bytes the fused kernel needs for a job with T threads.
 size_t fused_smem_bytes(const PtJob& j, uint32_t T, bool csr_smem);
