@@ -229,9 +229,39 @@ __device__ __forceinline__ MscLevels msc_levels(uint32_t S0, const uint32_t* Wj,
   return L;
 }
 
+// Four comparison levels k = 4 kk .. 4 kk + 3 of one word: level k compares
+// random word k (component k % 4 of Philox call kk) with threshold plane
+// 31 - k.  The four planes of a level group are one aligned 16-byte load
+// (planes 28 - 4 kk .. 31 - 4 kk; `pl` 16-byte aligned).
+template <uint32_t DEG>
+__device__ __forceinline__ void msc_step4(uint4 r, const uint32_t* pl, const MscLevels& L, uint32_t kk, uint32_t& und,
+                                          uint32_t& lt) {
+  constexpr uint32_t LV = DEG / 2;
+  uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+#pragma unroll
+  for (uint32_t l = 0; l < LV; ++l) {
+    const uint4 P = *reinterpret_cast<const uint4*>(pl + l * 32 + 28 - 4 * kk);
+    t0 |= P.w & L.lv[l];
+    t1 |= P.z & L.lv[l];
+    t2 |= P.y & L.lv[l];
+    t3 |= P.x & L.lv[l];
+  }
+  lt |= und & ~r.x & t0;
+  und &= ~(r.x ^ t0);
+  lt |= und & ~r.y & t1;
+  und &= ~(r.y ^ t1);
+  lt |= und & ~r.z & t2;
+  und &= ~(r.z ^ t2);
+  lt |= und & ~r.w & t3;
+  und &= ~(r.w ^ t3);
+}
+
 // The flip mask of one word: `pl` = threshold planes [DEG/2][32] of the word,
 // `al` / `nv` = replicas whose level always / never flips ([DEG/2]); random
 // words from Philox keyed by `key` and counted by (s, i, (wo << 8) | call).
+// Levels run in groups of four (one Philox call each) until no replica is
+// undecided; a replica decided within a group is untouched by its remaining
+// levels, so the result is the one of a level-by-level loop.
 template <uint32_t DEG>
 __device__ __forceinline__ uint32_t msc_flip(const MscLevels& L, const uint32_t* pl, const uint32_t* al,
                                              const uint32_t* nv, uint32_t s, uint32_t i, uint32_t wo, uint2 key) {
@@ -244,22 +274,14 @@ __device__ __forceinline__ uint32_t msc_flip(const MscLevels& L, const uint32_t*
     und |= L.lv[l] & ~al[l] & ~nv[l];
   }
   uint32_t lt = 0;
-  uint4 r = make_uint4(0, 0, 0, 0);
-  for (uint32_t k = 0; k < 32 && und; ++k) {
-    if ((k & 3u) == 0) r = philox4x32_10(make_uint4(s, i, (wo << 8) | (k >> 2), PTAG_MSC), key);
-    const uint32_t R = (k & 3u) == 0 ? r.x : (k & 3u) == 1 ? r.y : (k & 3u) == 2 ? r.z : r.w;
-    uint32_t t = 0;
-#pragma unroll
-    for (uint32_t l = 0; l < LV; ++l) t |= pl[l * 32 + (31 - k)] & L.lv[l];
-    lt |= und & ~R & t;
-    und &= ~(R ^ t);
-  }
+  for (uint32_t kk = 0; kk < 8 && und; ++kk)
+    msc_step4<DEG>(philox4x32_10(make_uint4(s, i, (wo << 8) | kk, PTAG_MSC), key), pl, L, kk, und, lt);
   return ~uphill | always | lt;
 }
 
 // msc_flip for two words of the same site at once (words wo and wo + 1, each
-// with its own planes and random words): the same decisions, with the two
-// random streams interleaved so that their Philox rounds overlap.
+// with its own planes and random words): the same decisions, with both Philox
+// calls of a level group issued together so that their rounds overlap.
 template <uint32_t DEG>
 __device__ __forceinline__ void msc_flip2(const MscLevels& L0, const MscLevels& L1, const uint32_t* pl0,
                                           const uint32_t* pl1, uint32_t s, uint32_t i, uint32_t wo, uint2 key,
@@ -277,25 +299,11 @@ __device__ __forceinline__ void msc_flip2(const MscLevels& L0, const MscLevels& 
     und1 |= L1.lv[l] & ~al1[l] & ~nv1[l];
   }
   uint32_t lt0 = 0, lt1 = 0;
-  uint4 r0 = make_uint4(0, 0, 0, 0), r1 = r0;
-  for (uint32_t k = 0; k < 32 && (und0 | und1); ++k) {
-    if ((k & 3u) == 0) {
-      if (und0) r0 = philox4x32_10(make_uint4(s, i, (wo << 8) | (k >> 2), PTAG_MSC), key);
-      if (und1) r1 = philox4x32_10(make_uint4(s, i, ((wo + 1) << 8) | (k >> 2), PTAG_MSC), key);
-    }
-    const uint32_t q = k & 3u;
-    const uint32_t R0 = q == 0 ? r0.x : q == 1 ? r0.y : q == 2 ? r0.z : r0.w;
-    const uint32_t R1 = q == 0 ? r1.x : q == 1 ? r1.y : q == 2 ? r1.z : r1.w;
-    uint32_t t0 = 0, t1 = 0;
-#pragma unroll
-    for (uint32_t l = 0; l < LV; ++l) {
-      t0 |= pl0[l * 32 + (31 - k)] & L0.lv[l];
-      t1 |= pl1[l * 32 + (31 - k)] & L1.lv[l];
-    }
-    lt0 |= und0 & ~R0 & t0;
-    und0 &= ~(R0 ^ t0);
-    lt1 |= und1 & ~R1 & t1;
-    und1 &= ~(R1 ^ t1);
+  for (uint32_t kk = 0; kk < 8 && (und0 | und1); ++kk) {
+    const uint4 r0 = philox4x32_10(make_uint4(s, i, (wo << 8) | kk, PTAG_MSC), key);
+    const uint4 r1 = philox4x32_10(make_uint4(s, i, ((wo + 1) << 8) | kk, PTAG_MSC), key);
+    msc_step4<DEG>(r0, pl0, L0, kk, und0, lt0);
+    msc_step4<DEG>(r1, pl1, L1, kk, und1, lt1);
   }
   f0 = ~up0 | alw0 | lt0;
   f1 = ~up1 | alw1 | lt1;

@@ -137,8 +137,11 @@ __host__ __device__ inline size_t xchg_layout(XchgSm* X, char* base, uint32_t C,
   return o;
 }
 
-// words of multi-spin-coding thresholds per replica word (levels x < 3)
-constexpr uint32_t MSC_WORDS = 3 * 32 + 3 + 3;
+// words of multi-spin-coding thresholds per replica word (levels x < 3):
+// [3][32] planes, [3] always, [3] never, padded so that every word's planes
+// start on a 16-byte boundary (msc_step4 loads four planes at once)
+constexpr uint32_t MSC_WORDS = 3 * 32 + 3 + 3 + 2;
+static_assert(MSC_WORDS % 4 == 0, "16-byte aligned threshold planes");
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
 
@@ -149,9 +152,12 @@ __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~(size_t)15
 //   ICM_BFS_ONE  (one slot) the queue of visited sites [n] u32.
 enum { ICM_UF = 0, ICM_BFS = 1, ICM_BFS_ONE = 2 };
 __host__ __device__ inline size_t icm_n16(uint32_t n) { return ((size_t)n + 7) / 8 * 8; }
+// (ICM_UF and ICM_BFS also hold the several-slot seed scan's transposed chunk
+// masks first: at least 32 words per chunk of 32 sites.)
 __host__ __device__ inline size_t icm_label_words(uint32_t n, uint32_t G, int mode) {
-  if (mode == ICM_UF) return (size_t)G * n;
-  if (mode == ICM_BFS) return (size_t)n + 3 * icm_n16(n) / 2;
+  const size_t chunks = ((size_t)n + 31) / 32 * 32;
+  if (mode == ICM_UF) return (size_t)G * n > chunks ? (size_t)G * n : chunks;
+  if (mode == ICM_BFS) return (size_t)n + 3 * icm_n16(n) / 2 > chunks ? (size_t)n + 3 * icm_n16(n) / 2 : chunks;
   return n;
 }
 
@@ -440,6 +446,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
   // replica 0's words, read once (kept in shared memory when W is not); the
   // energy change needs no other replica words
   auto r0 = [&](uint32_t s) -> uint32_t { return wstage ? wstage[s] : W[s * nw + o0]; };
+  if (pc) pc->lap(PHASE_OTHER);
   for (uint32_t s = tid; s < n; s += T) {
     const uint32_t v0 = W[s * nw + o0], v1 = W[s * nw + o1];
     if (wstage) wstage[s] = v0;
@@ -455,6 +462,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
   }
   if (tid < 64) X.dE[tid] = 0;
   __syncthreads();
+  if (pc && !uf) pc->lap(PHASE_ICM_INIT);
   const uint32_t G = __popc(gmask);
   if (G == 1) {
     // one slot: each warp counts a contiguous segment of sites with ballots,
@@ -497,56 +505,60 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
       if (tid == 0) X.cnt[b] = cnt;
     }
   } else {
-    // several slots: one warp per slot, ballot scans in site order.  Up to 32
-    // chunks of 32 sites, lane L keeps chunk L's count, and a prefix sum over the
-    // lanes finds the chunk of the k-th site (no second scan)
+    // several slots: the (gmask-masked) disagreement words of 32 consecutive
+    // sites are transposed in a warp, so lane b holds slot b's bits of those
+    // sites; the masks go to XL as [chunk][32].  Then one warp per slot counts
+    // its sites (lane = chunk, in groups of 32 chunks), draws k and finds the
+    // chunk holding the k-th site by a prefix sum over the lanes and the site
+    // by __fns: the site a scan in site order would find.
     const uint32_t nchunk = (n + 31) / 32;
+    uint32_t* const M = XL;  // 32 * nchunk words (icm_label_words)
+    for (uint32_t ch = warp; ch < nchunk; ch += nwarp) {
+      const uint32_t s = ch * 32 + lane;
+      M[ch * 32 + lane] = transpose32(s < n ? XD[s] : 0u, lane);
+    }
+    __syncthreads();
     for (uint32_t b = warp; b < 32; b += nwarp) {
       if (!((gmask >> b) & 1u)) continue;
       const uint32_t u = philox4x32_10(make_uint4(tb + b, i, p, PTAG_ICM), J.key).x;  // needed only if cnt > 0
-      uint32_t cnt = 0, cc = 0;
-#pragma unroll 4
-      for (uint32_t ch = 0; ch < nchunk; ++ch) {
-        const uint32_t s = ch * 32 + lane;
-        const uint32_t c = __popc(__ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u)));
-        cnt += c;
-        if (ch == lane) cc = c;
+      uint32_t cnt = 0;
+      for (uint32_t c0 = 0; c0 < nchunk; c0 += 32) {
+        const uint32_t ch = c0 + lane;
+        cnt += ch < nchunk ? (uint32_t)__popc(M[ch * 32 + b]) : 0u;
       }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
       if (cnt == 0) continue;
       uint32_t k = (uint32_t)(((uint64_t)u * cnt) >> 32);
-      if (nchunk <= 32) {
+      for (uint32_t c0 = 0; c0 < nchunk; c0 += 32) {
+        const uint32_t ch = c0 + lane;
+        const uint32_t m = ch < nchunk ? M[ch * 32 + b] : 0u;
+        const uint32_t cc = __popc(m);
         uint32_t incl = cc;
+#pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
           const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
           if (lane >= (uint32_t)o) incl += v;
         }
-        const uint32_t excl = incl - cc;
-        const uint32_t ch = __ffs(__ballot_sync(0xffffffffu, k >= excl && k < incl)) - 1;  // exactly one chunk
-        const uint32_t kk = k - __shfl_sync(0xffffffffu, excl, ch);
-        const uint32_t s = ch * 32 + lane;
-        const uint32_t bal = __ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u));
-        if (lane == 0) {
-          X.seed[b] = ch * 32 + __fns(bal, 0, (int)kk + 1);
-          X.cnt[b] = cnt;
-        }
-        continue;
-      }
-      for (uint32_t base = 0; base < n; base += 32) {
-        const uint32_t s = base + lane;
-        const uint32_t bal = __ballot_sync(0xffffffffu, s < n && ((XD[s] >> b) & 1u));
-        const uint32_t c = __popc(bal);
-        if (k < c) {
-          if (lane == 0) {
-            X.seed[b] = base + __fns(bal, 0, (int)k + 1);
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        if (k < tot) {  // warp-uniform
+          const uint32_t excl = incl - cc;
+          if (k >= excl && k < incl) {  // exactly one lane
+            X.seed[b] = ch * 32 + __fns(m, 0, (int)(k - excl) + 1);
             X.cnt[b] = cnt;
           }
           break;
         }
-        k -= c;
+        k -= tot;
       }
     }
   }
   __syncthreads();
+  if (!PLAIN && G > 1 && !uf && !prop) {
+    // the breadth-first search's level marks, which the scan's masks overwrote
+    for (uint32_t s = tid; s < n; s += T) XL[s] = 0;
+    __syncthreads();
+  }
   if (pc) pc->lap(PHASE_ICM_SCAN);
   auto col = [&](uint32_t e) -> uint32_t { return cols ? cols[e] : ent[e].x; };
   // BFS: the cluster sites (16-bit list for several slots, 32-bit for one);
@@ -2241,7 +2253,7 @@ __global__ void __launch_bounds__(256, 3) k_plain_sweep(const PtJob* __restrict_
 // words, so both forms stay identical.  Per-replica energy sums: bit
 // transposes per warp, then one 64-bit atomic per replica and CTA.
 template <uint32_t DEG, bool CLOSE>
-__global__ void __launch_bounds__(256, 4) k_plain_sweep_msc(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
+__global__ void __launch_bounds__(256, 3) k_plain_sweep_msc(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
                                                          long long* acc) {
   extern __shared__ uint4 smem_u4[];
   const PtJob& J = *jp;
