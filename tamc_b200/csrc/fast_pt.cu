@@ -944,15 +944,22 @@ __device__ void icm_phase(const PtJob& J, const FastInst& F, Smem& S, uint32_t i
     const uint32_t c0 = 2 * p, c1 = 2 * p + 1;
     for (uint32_t w = 0; w < J.wpc; ++w) {
       const uint32_t tb = 32 * w;
-      uint32_t lomask = 0;
-      for (uint32_t b = 0; b < 32; ++b)
-        if (tb + b >= J.lo && tb + b < J.nt) lomask |= 1u << b;
+      // slots lo <= tb + b < nt of this word
+      const uint32_t lo_b = J.lo > tb ? min(J.lo - tb, 32u) : 0u;
+      const uint32_t hi_b = J.nt > tb ? min(J.nt - tb, 32u) : 0u;
+      const uint32_t below_hi = hi_b >= 32 ? 0xffffffffu : (1u << hi_b) - 1u;
+      const uint32_t below_lo = lo_b >= 32 ? 0xffffffffu : (1u << lo_b) - 1u;
+      uint32_t lomask = below_hi & ~below_lo;
       while (lomask) {
         // next group: the lowest `icm_group` set bits
-        uint32_t gmask = 0, m = lomask;
-        for (uint32_t g = 0; g < J.icm_group && m; ++g) {
-          gmask |= m & (~m + 1u);
-          m &= m - 1;
+        uint32_t gmask = lomask;
+        if ((uint32_t)__popc(lomask) > J.icm_group) {
+          gmask = 0;
+          uint32_t m = lomask;
+          for (uint32_t g = 0; g < J.icm_group && m; ++g) {
+            gmask |= m & (~m + 1u);
+            m &= m - 1;
+          }
         }
         lomask &= ~gmask;
         icm_group<false>(J, F, S.W, S.X, i, p, w, gmask, nullptr, nullptr, &pc);
