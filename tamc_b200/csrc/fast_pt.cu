@@ -926,6 +926,7 @@ __device__ void icm_group(const PtJob& J, const FastInst& F, uint32_t* W, IcmScr
       __syncthreads();
     }
   }
+  if (pc && prop) pc->lap(PHASE_ICM_MARK);  // (propagation: the energy change ends here, the flip follows)
   for (uint32_t x = tid; x < nlist; x += T) {
     const uint32_t s = vlist ? vlist[x] : vlist16 ? (uint32_t)vlist16[x] : x;
     const uint32_t c = XC[s];
@@ -1471,7 +1472,7 @@ __device__ __forceinline__ void load_job(PtJob& dst, const PtJob* src) {
 
 // The fused job's bookkeeping into shared memory (start of a range of rounds)
 // and back (its end); the end also reports the log count.
-__device__ __noinline__ void xchg_load(const PtJob& J, char* xb) {
+__device__ __noinline__ void xchg_load(const PtJob& J, char* xb, bool gs = true) {
   XchgSm X;
   xchg_layout(&X, xb, J.C, J.ntp);
   const uint32_t CT = J.C * J.nt;
@@ -1483,14 +1484,14 @@ __device__ __noinline__ void xchg_load(const PtJob& J, char* xb) {
   }
   for (uint32_t c = threadIdx.x; c < J.C; c += blockDim.x) X.rtrips[c] = J.rtrips[c];
   for (uint32_t j = threadIdx.x; j + 1 < J.nt; j += blockDim.x) X.dbeta[j] = J.betas[j + 1] - J.betas[j];
-  if (threadIdx.x == 0) {
+  if (gs && threadIdx.x == 0) {
     X.gs->have = *J.log.have;
     X.gs->minE = *J.log.minE;
     X.gs->count = *J.log.count;
   }
   __syncthreads();
 }
-__device__ __noinline__ void xchg_store(const PtJob& J, char* xb) {
+__device__ __noinline__ void xchg_store(const PtJob& J, char* xb, bool gs = true) {
   XchgSm X;
   xchg_layout(&X, xb, J.C, J.ntp);
   const uint32_t CT = J.C * J.nt;
@@ -1501,7 +1502,7 @@ __device__ __noinline__ void xchg_store(const PtJob& J, char* xb) {
     J.dhist[2 * x + 1] = X.dhist[2 * x + 1];
   }
   for (uint32_t c = threadIdx.x; c < J.C; c += blockDim.x) J.rtrips[c] = X.rtrips[c];
-  if (threadIdx.x == 0) {
+  if (gs && threadIdx.x == 0) {
     *J.log.have = X.gs->have;
     *J.log.minE = X.gs->minE;
     *J.log.count = X.gs->count;
@@ -1619,6 +1620,11 @@ __global__ void __launch_bounds__(512, 1) k_pt_fused(const PtJob* __restrict__ j
 __host__ __device__ inline size_t plain_head_smem(uint32_t n, uint32_t C, uint32_t ntp) {
   (void)n;
   return al16((size_t)C * ntp * 8) * 2 + al16((size_t)C * 8) + 64;
+}
+// The exchange body's shared memory: the head's energies and masks, then the
+// bookkeeping staged from global memory (XchgSm).
+__host__ __device__ inline size_t plain_exch_smem(uint32_t n, uint32_t C, uint32_t ntp) {
+  return plain_head_smem(n, C, ntp) + xchg_layout(nullptr, nullptr, C, ntp);
 }
 
 // Close the previous round (add its fixed-point sweep sums, measurements), or
@@ -2066,10 +2072,15 @@ __device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long lo
     S.Er[x] = er;
   }
   __syncthreads();
+  // the exchange bookkeeping in shared memory: one round of parallel global
+  // loads and stores instead of dependent global round trips in the decisions
+  S.xb = base + plain_head_smem(J.n, J.C, J.ntp);
+  xchg_load(J, S.xb, false);
   PhaseClock pc;
   pc.start(J.prof);
   const uint32_t i = ctl->i;
   exchange_decide(J, S, i);
+  xchg_store(J, S.xb, false);
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
     J.Ec[x] = S.Ec[x];
     J.Er[x] = S.Er[x];
@@ -2406,7 +2417,7 @@ static size_t plain_icm_smem(const PtJob& j, int stage) {
   size_t b = carve_icm(nullptr, nullptr, 0, j.n, 1, j.icm_uf ? ICM_UF : ICM_BFS_ONE);
   if (stage & 2) b += al16((size_t)j.n * 4);
   if (stage & 1) b += al16((size_t)(j.n + 1) * 4) + al16((size_t)j.F.nnz * 2);
-  return std::max(b, plain_head_smem(j.n, j.C, j.ntp));
+  return std::max(b, plain_exch_smem(j.n, j.C, j.ntp));
 }
 size_t plain_icm_bytes(const PtJob& j) { return plain_icm_smem(j, 0); }
 
@@ -2460,7 +2471,7 @@ static bool plain_launch_icm_cluster(cudaStream_t st, const PtJob& j, const PtJo
     if (ps > 2) continue;  // more sites per thread spill at 64 registers
     const uint32_t psr = ps <= 1 ? 1 : 2;
     const size_t smem = std::max(carve_icm_cl(nullptr, nullptr, j.n, T, psr, deg, CL),
-                                 plain_head_smem(j.n, j.C, j.ntp));
+                                 plain_exch_smem(j.n, j.C, j.ntp));
     if (smem > smem_limit) continue;
     if (CL == 4) {
       if (deg == 4) launch_icm_cl_ps<4, 4>(st, psr, nclusters, smem, d_job, ctl, icm_dE, icm_valid, dm);
@@ -2492,7 +2503,7 @@ bool plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, Plain
 
 void plain_launch_exch(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, const long long* icm_dE,
                        uint32_t* icm_valid, unsigned long long* dm) {
-  const size_t smem = plain_head_smem(j.n, j.C, j.ntp);
+  const size_t smem = plain_exch_smem(j.n, j.C, j.ntp);
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_exch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_plain_exch<<<1, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, dm);
   TAMC_CUDA(cudaGetLastError());
