@@ -105,6 +105,40 @@ void free_all_locked(DevCache& C) {
   C.pending.clear();
   C.bytes = 0;
 }
+
+// Side L when the coupling graph is exactly the periodic square (d = 2) or
+// cubic (d = 3) lattice of side 16 or 32 in the file's site order (site
+// x L^2 + y L + z, z fastest; every row the 2d neighbours at +-1 along each
+// axis modulo L, in any order, no self-coupling), else 0.  Rows of such a
+// lattice fill half or whole 32-bit words, which the plain form's bitmap
+// Houdayer search relies on.
+uint32_t lattice_side(const HostInstance& h, uint32_t udeg) {
+  if (udeg != 4 && udeg != 6) return 0;
+  const uint32_t d = udeg / 2;
+  for (uint32_t L : {16u, 32u}) {
+    const uint64_t n = d == 2 ? (uint64_t)L * L : (uint64_t)L * L * L;
+    if (n != h.n) continue;
+    for (uint32_t i = 0; i < h.n; ++i) {
+      const uint32_t r0 = h.row_ptr[i], r1 = h.row_ptr[i + 1];
+      if (r1 - r0 != udeg) return 0;
+      uint32_t want[6];
+      uint32_t k = 0, stride = 1;
+      for (uint32_t a = 0; a < d; ++a, stride *= L) {
+        const uint32_t c = (i / stride) % L;
+        want[k++] = i - c * stride + ((c + 1) % L) * stride;
+        want[k++] = i - c * stride + ((c + L - 1) % L) * stride;
+      }
+      std::sort(want, want + udeg);
+      uint32_t got[6];
+      for (uint32_t e = 0; e < udeg; ++e) got[e] = h.col[r0 + e];
+      std::sort(got, got + udeg);
+      for (uint32_t e = 0; e < udeg; ++e)
+        if (got[e] != want[e]) return 0;
+    }
+    return L;
+  }
+  return 0;
+}
 }  // namespace
 
 void* dev_alloc(size_t bytes) {
@@ -363,6 +397,24 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
       if (fbias[s] != 0.0f) d->pmj = 0;
     for (size_t e = 0; e < fent.size() && d->pmj; ++e)
       if ((fent[e].y & 0x7fffffffu) != 0x3f800000u) d->pmj = 0;  // |J| == 1.0f
+    d->lat_L = lattice_side(h, d->udeg);
+    std::vector<float> fJt;
+    std::vector<uint16_t> fcolt;
+    if (d->lat_L) {
+      // couplings and columns by (neighbour slot, colour row) for the bitmap
+      // Houdayer kernel: contiguous 16-byte staging, conflict-free reads of
+      // the m-th entries of consecutive rows
+      const uint32_t D = d->udeg;
+      fJt.resize(fent.size());
+      fcolt.resize(fent.size());
+      for (uint32_t s = 0; s < h.n; ++s)
+        for (uint32_t m = 0; m < D; ++m) {
+          memcpy(&fJt[(size_t)m * h.n + s], &fent[(size_t)s * D + m].y, 4);
+          fcolt[(size_t)m * h.n + s] = (uint16_t)fent[(size_t)s * D + m].x;
+        }
+      pack.add(&d->d_fJt, fJt.data(), fJt.size());
+      pack.add(&d->d_fcolt, fcolt.data(), fcolt.size());
+    }
     pack.add(&d->d_fbias, fbias.data(), fbias.size());
     pack.add(&d->d_fkd, fkd.data(), fkd.size());
     pack.add(&d->d_fsus, fsus.data(), fsus.size());

@@ -233,9 +233,12 @@ struct tamc_inst {
   uint32_t* d_iperm = nullptr;       // original -> new
   uint32_t* d_frp = nullptr;         // n + 1
   uint2* d_fent = nullptr;           // nnz (col_new, J bits)
+  float* d_fJt = nullptr;            // lattice instances: couplings [udeg][n] (entry m of colour row s at m n + s)
+  uint16_t* d_fcolt = nullptr;       // lattice instances: columns [udeg][n], same layout
   uint16_t* d_fcol16 = nullptr;      // nnz col_new as 16 bits, padded to 8 entries (n <= 65536 only)
   uint32_t udeg = 0;                 // entries per row when every row has the same count, else 0
   int pmj = 0;                       // +-1 couplings, no field, no self-loop, rows of 4 or 6 entries
+  uint32_t lat_L = 0;                // periodic L^d lattice in file order (L 16 or 32, d = udeg / 2), else 0
   float* d_fbias = nullptr;          // n
   void* arena = nullptr;             // one allocation holding every array above
   size_t arena_bytes = 0;

@@ -23,6 +23,9 @@ struct FastInst {  // colour-ordered instance (device pointers)
   const uint16_t* col16;      // nnz new column as 16 bits, padded to 8 entries; null if n > 65536
   uint32_t udeg;              // entries per row if uniform (row s = [s*udeg, (s+1)*udeg)), else 0
   int pmj;                    // +-1 couplings, zero field, no self-loop, udeg 4 or 6 (multi-spin coding)
+  uint32_t lat_L;             // side of a periodic square / cubic lattice in file order (16 or 32), else 0
+  const float* fJt;           // lattice instances: couplings [udeg][n] (entry m of colour row s at m n + s)
+  const uint16_t* fcolt;      // lattice instances: columns [udeg][n], same layout
   const float* bias;          // n
   const float* kd;            // n self-loop coefficient
   const double* sus;          // [nchi][n], colour order

@@ -1784,6 +1784,345 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__
   plain_exchange_body(J, ctl, icm_dE, icm_valid, base, dm);
 }
 
+// Houdayer moves of round ctl->i on a periodic square or cubic lattice of
+// side L = 16 or 32 in file order (FastInst::lat_L): one CTA per (chain pair,
+// slot >= lo), as k_plain_icm, with the slot's disagreement set and cluster
+// held as bitmaps over the original site order (n / 32 words; a lattice row
+// fills half or all of a word).  A growth pass is word-parallel: each of the
+// first n / 32 threads owns one word and first closes it under the moves
+// inside the word (z +-1 within each row; for L = 16 also between the word's
+// two rows), then adds the D sites next to cluster sites of the words of the
+// neighbouring rows and planes; a warp repeats this while its words grow, and
+// passes (a barrier over the growth threads) end when one changes nothing, so
+// the result is the exact component of the seed.  Meanwhile the other threads
+// stage the couplings, columns, fields and permutation for the energy change.  The seed is the k-th q<0 site
+// in colour order with k drawn as in icm_group, and the energy change sums
+// each cluster site's boundary terms in its colour-ordered row order with the
+// couplings and columns staged in shared memory, so the move, the flips and
+// the fixed-point sums are those of k_plain_icm bit for bit.
+struct LatScratch {
+  float* Jf;         // [DEG][n] couplings: entry m of colour row s at m n + s
+  uint16_t* cols;    // [DEG][n] columns, same layout
+  uint32_t* Dcol;    // [NW] q<0 bits of the slot, colour order
+  uint32_t* R0col;   // [NW] replica 0's spin bits of the slot, colour order
+  uint32_t* Do;      // [NW] q<0 bits, original order
+  uint32_t* Co;      // [NW] cluster bits, original order
+  uint32_t* Ccol;    // [NW] cluster bits, colour order
+  float* bias;       // [n] fields, colour order
+  uint32_t* perm;    // [n] colour -> file order
+  long long* part;   // [32] per-warp energy sums
+  uint32_t* misc;    // [4] seed count, seed site, pass flag
+};
+__host__ __device__ inline size_t carve_lat(LatScratch* X, char* base, uint32_t n, uint32_t nnz) {
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    char* p = base ? base + o : nullptr;
+    o = al16(o + bytes);
+    return p;
+  };
+  const size_t NW = (n + 31) / 32;
+  char* Jf = take((size_t)nnz * 4);
+  char* cols = take((size_t)nnz * 2);
+  char* Dcol = take(NW * 4);
+  char* R0col = take(NW * 4);
+  char* Do = take(NW * 4);
+  char* Co = take(NW * 4);
+  char* Ccol = take(NW * 4);
+  char* bias = take((size_t)n * 4);
+  char* perm = take((size_t)n * 4);
+  char* part = take(32 * 8);
+  char* misc = take(4 * 4);
+  if (X) {
+    X->Jf = (float*)Jf;
+    X->cols = (uint16_t*)cols;
+    X->Dcol = (uint32_t*)Dcol;
+    X->R0col = (uint32_t*)R0col;
+    X->Do = (uint32_t*)Do;
+    X->Co = (uint32_t*)Co;
+    X->Ccol = (uint32_t*)Ccol;
+    X->bias = (float*)bias;
+    X->perm = (uint32_t*)perm;
+    X->part = (long long*)part;
+    X->misc = (uint32_t*)misc;
+  }
+  return o;
+}
+
+// Closure of the cluster bits c under the moves inside one bitmap word of the
+// q<0 bits d: along each row (periodic in L), and for L = 16 between the
+// word's two rows.  A row is filled from its seeds with one addition each
+// way: on the row written twice in a row, the carry of d + c runs from every
+// seed through the run of d above it (past the row's end into the copy: the
+// periodic wrap), and bit reversal gives the other direction.
+__device__ __forceinline__ uint32_t lat_fill32(uint32_t c, uint32_t d) {
+  const uint64_t dd = (uint64_t)d | ((uint64_t)d << 32);
+  uint64_t up = (((dd + c) ^ dd) & dd) | c;
+  const uint32_t rd = __brev(d), rc = __brev(c);
+  const uint64_t rdd = (uint64_t)rd | ((uint64_t)rd << 32);
+  uint64_t dn = (((rdd + rc) ^ rdd) & rdd) | rc;
+  return (uint32_t)(up | (up >> 32)) | __brev((uint32_t)(dn | (dn >> 32)));
+}
+__device__ __forceinline__ uint32_t lat_fill16(uint32_t c, uint32_t d) {  // c, d < 2^16
+  const uint32_t dd = d | (d << 16);
+  uint32_t up = (((dd + c) ^ dd) & dd) | c;
+  const uint32_t rd = __brev(dd), rc = __brev(c) >> 16;
+  uint32_t dn = (((rd + rc) ^ rd) & rd) | rc;
+  return ((up | (up >> 16)) & 0xffffu) | (__brev((dn | (dn >> 16)) & 0xffffu) >> 16);
+}
+// (For L = 16 two rounds of row fill and row coupling, a fixed cost per call:
+// what remains to couple is added by the next call of the growth loop.)
+__device__ __forceinline__ uint32_t lat_fill_rows16(uint32_t c, uint32_t d) {
+  return lat_fill16(c & 0xffffu, d & 0xffffu) | (lat_fill16(c >> 16, d >> 16) << 16);
+}
+template <uint32_t L>
+__device__ __forceinline__ uint32_t lat_close(uint32_t c, uint32_t d) {
+  if (L == 32) return lat_fill32(c, d);
+  c = lat_fill_rows16(c, d);
+  c |= d & ((c >> 16) | (c << 16));  // the word's two rows are neighbours
+  c = lat_fill_rows16(c, d);
+  return c | (d & ((c >> 16) | (c << 16)));
+}
+
+// Barrier over the first `count` threads (a multiple of 32) on barrier 1,
+// returning whether any of them passed a non-zero `pred`.
+__device__ __forceinline__ int bar1_or(int pred, uint32_t count) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 q, %1, 0;\n\tbar.red.or.pred p, 1, %2, q;\n\tselp.s32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"(pred), "r"(count)
+      : "memory");
+  return r;
+}
+
+template <uint32_t L, uint32_t DIM>
+__global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restrict__ jp, PlainCtl* ctl,
+                                                           long long* icm_dE, uint32_t* icm_valid,
+                                                           unsigned long long* dm) {
+  extern __shared__ uint4 smem_u4[];
+  __shared__ PtJob s_J;
+  load_job(s_J, jp);
+  const PtJob& J = s_J;
+  constexpr uint32_t DEG = 2 * DIM;
+  constexpr uint32_t n = DIM == 2 ? L * L : L * L * L;
+  constexpr uint32_t NW = n / 32;                  // bitmap words
+  constexpr uint32_t WPP = L * L / 32;             // words per plane of L rows
+  constexpr uint32_t G = (NW + 31) / 32 * 32;      // threads of the growth group
+  static_assert(G < 1024, "the growth group leaves threads for the staging");
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  const uint32_t T = blockDim.x;
+  const uint32_t nact = J.nt - J.lo;
+  const uint32_t p = blockIdx.x / nact, t = J.lo + blockIdx.x % nact;
+  const uint32_t b = t & 31u, w = t >> 5, tb = 32 * w;
+  const uint32_t nw = J.nw, o0 = 2 * p * J.wpc + w, o1 = (2 * p + 1) * J.wpc + w;
+  const uint32_t nnz = J.F.nnz;
+  char* base = reinterpret_cast<char*>(smem_u4);
+  LatScratch X;
+  carve_lat(&X, base, n, nnz);
+  uint32_t* const Wg = J.W;
+  PhaseClock pc;  // with profiling on, cycles are summed over the CTAs
+  pc.start(J.prof);
+  // the slot's q<0 bits and replica 0's spin bits in colour order (ballots;
+  // a warp's words at most NW / 32 <= 4, their loads issued together)
+  constexpr uint32_t WPW = NW >= 32 * 32 ? 32 : (NW + 31) / 32;  // words per warp
+  {
+    uint32_t v0[WPW], v1[WPW];
+#pragma unroll
+    for (uint32_t k = 0; k < WPW; ++k) {
+      const uint32_t wc = warp + k * nwarp;
+      const uint32_t s = 32 * wc + lane;
+      v0[k] = wc < NW ? Wg[(size_t)s * nw + o0] : 0u;
+      v1[k] = wc < NW ? Wg[(size_t)s * nw + o1] : 0u;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < WPW; ++k) {
+      const uint32_t wc = warp + k * nwarp;
+      const uint32_t dq = __ballot_sync(0xffffffffu, ((v0[k] ^ v1[k]) >> b) & 1u);
+      const uint32_t r0 = __ballot_sync(0xffffffffu, (v0[k] >> b) & 1u);
+      if (lane == 0 && wc < NW) {
+        X.Dcol[wc] = dq;
+        X.R0col[wc] = r0;
+      }
+    }
+  }
+  uint32_t ip[WPW];  // file order -> colour order of this lane's sites
+#pragma unroll
+  for (uint32_t k = 0; k < WPW; ++k) {
+    const uint32_t wo = warp + k * nwarp;
+    ip[k] = wo < NW ? J.F.iperm[32 * wo + lane] : 0u;
+  }
+  __syncthreads();
+  // the q<0 bits in original order; the cluster starts empty
+#pragma unroll
+  for (uint32_t k = 0; k < WPW; ++k) {
+    const uint32_t wo = warp + k * nwarp;
+    const uint32_t s = ip[k];
+    const uint32_t dq = __ballot_sync(0xffffffffu, wo < NW && ((X.Dcol[s >> 5] >> (s & 31u)) & 1u));
+    if (lane == 0 && wo < NW) {
+      X.Do[wo] = dq;
+      X.Co[wo] = 0;
+    }
+  }
+  // seed (warp 0): the k-th q<0 site in colour order, k = floor(u cnt / 2^32)
+  if (warp == 0) {
+    uint32_t cnt = 0;
+    for (uint32_t c0 = 0; c0 < NW; c0 += 32)
+      cnt += c0 + lane < NW ? (uint32_t)__popc(X.Dcol[c0 + lane]) : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    uint32_t seed = 0xffffffffu;
+    if (cnt) {
+      const uint32_t u = philox4x32_10(make_uint4(tb + b, ctl->i, p, PTAG_ICM), J.key).x;
+      uint32_t k = (uint32_t)(((uint64_t)u * cnt) >> 32);
+      for (uint32_t c0 = 0; c0 < NW; c0 += 32) {
+        const uint32_t m = c0 + lane < NW ? X.Dcol[c0 + lane] : 0u;
+        const uint32_t cc = __popc(m);
+        uint32_t incl = cc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= (uint32_t)o) incl += v;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        if (k < tot) {
+          const uint32_t excl = incl - cc;
+          const uint32_t hit = __ballot_sync(0xffffffffu, k >= excl && k < incl);
+          const uint32_t src = __ffs(hit) - 1;
+          seed = (c0 + src) * 32 + __fns(__shfl_sync(0xffffffffu, m, src), 0,
+                                         (int)(k - __shfl_sync(0xffffffffu, excl, src)) + 1);
+          break;
+        }
+        k -= tot;
+      }
+    }
+    if (lane == 0) {
+      X.misc[0] = cnt;
+      X.misc[1] = seed;
+    }
+  }
+  __syncthreads();
+  pc.lap(PHASE_ICM_SCAN);
+  const uint32_t cnt = X.misc[0];
+  if (tid < G) {
+    // growth group: thread tid owns bitmap word tid.  Inside a pass a warp
+    // repeats its words' updates while any of them grows (its words are
+    // neighbouring rows and planes), then the group's barrier
+    if (cnt && tid == 0) {
+      const uint32_t o = J.F.perm[X.misc[1]];
+      X.Co[o >> 5] = 1u << (o & 31u);
+    }
+    bar1_or(0, G);
+    const uint32_t wi = tid;
+    const bool own = cnt && wi < NW;
+    const uint32_t d = own ? X.Do[wi] : 0u;
+    uint32_t c = own ? X.Co[wi] : 0u;
+    const uint32_t j = wi % WPP, plane0 = wi - j;
+    const uint32_t wym = plane0 + (j + WPP - 1) % WPP, wyp = plane0 + (j + 1) % WPP;
+    const uint32_t wxm = (wi + NW - WPP) % NW, wxp = (wi + WPP) % NW;
+    for (uint32_t pass = 0; cnt && pass < n + 2u; ++pass) {
+      int grew = 0;
+      for (uint32_t rep = 0; rep < 64u; ++rep) {
+        int g = 0;
+        if (own && d != c) {
+          const uint32_t c_in = c;
+          c = lat_close<L>(c, d);  // closure inside the word
+          uint32_t nb = L == 16 ? (X.Co[wym] >> 16) | (X.Co[wyp] << 16) : X.Co[wym] | X.Co[wyp];
+          if (DIM == 3) nb |= X.Co[wxm] | X.Co[wxp];
+          c |= d & nb;
+          if (c != c_in) {
+            X.Co[wi] = c;
+            g = 1;
+          }
+        }
+        grew |= g;
+        if (!__any_sync(0xffffffffu, g)) break;
+        __syncwarp();
+      }
+      if (!bar1_or(grew, G)) break;
+    }
+  } else {
+    // staging group: couplings, columns, fields and the colour -> file order
+    // permutation into shared memory while the cluster grows
+    // (asynchronous 16-byte copies, all in flight at once)
+    const uint32_t st = tid - G, ns = T - G;
+    auto copy16 = [&](void* dst, const void* src, uint32_t n16) {
+      const uint32_t d0 = (uint32_t)__cvta_generic_to_shared(dst);
+      const char* s0 = static_cast<const char*>(src);
+      for (uint32_t x = st; x < n16; x += ns)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d0 + 16 * x), "l"(s0 + 16 * (size_t)x)
+                     : "memory");
+    };
+    copy16(X.Jf, J.F.fJt, nnz / 4);
+    copy16(X.cols, J.F.fcolt, nnz / 8);
+    copy16(X.bias, J.F.bias, n / 4);
+    copy16(X.perm, J.F.perm, n / 4);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+  }
+  __syncthreads();
+  pc.lap(PHASE_ICM_GROW);
+  long long a0 = 0;
+  if (cnt) {
+    // the cluster in colour order
+    for (uint32_t wc = warp; wc < NW; wc += nwarp) {
+      const uint32_t o = X.perm[32 * wc + lane];
+      const uint32_t cb = __ballot_sync(0xffffffffu, (X.Co[o >> 5] >> (o & 31u)) & 1u);
+      if (lane == 0) X.Ccol[wc] = cb;
+    }
+    __syncthreads();
+    // energy change of flipping the cluster in replica 0: boundary terms
+    // -2 s_i (h_i + sum_{j not in cluster} J_ij s_j), f32 in row order, summed
+    // in fixed point (replica 1's sum is the exact negative)
+    auto bit = [](const uint32_t* m, uint32_t s) { return (m[s >> 5] >> (s & 31u)) & 1u; };
+    for (uint32_t s = tid; s < n; s += T) {
+      if (!bit(X.Ccol, s)) continue;
+      float f0 = X.bias[s];
+#pragma unroll
+      for (uint32_t m = 0; m < DEG; ++m) {
+        const uint32_t jj = X.cols[m * n + s];
+        if (jj == s || bit(X.Ccol, jj)) continue;
+        const float Jv = X.Jf[m * n + s];
+        f0 += bit(X.R0col, jj) ? -Jv : Jv;
+      }
+      const float s0 = bit(X.R0col, s) ? -1.0f : 1.0f;
+      a0 += to_fx(-2.0f * s0 * f0);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+    if (lane == 0) X.part[warp] = a0;
+    __syncthreads();
+    a0 = 0;
+    for (uint32_t k = 0; k < nwarp; ++k) a0 += X.part[k];
+    pc.lap(PHASE_ICM_MARK);
+    // flip the cluster in both replicas
+    for (uint32_t s = tid; s < n; s += T)
+      if (bit(X.Ccol, s)) {
+        atomicXor(&Wg[(size_t)s * nw + o0], 1u << b);
+        atomicXor(&Wg[(size_t)s * nw + o1], 1u << b);
+      }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t x0 = 2 * p * J.ntp + t, x1 = (2 * p + 1) * J.ntp + t;
+    icm_valid[x0] = cnt != 0;
+    icm_valid[x1] = cnt != 0;
+    icm_dE[x0] = a0;
+    icm_dE[x1] = -a0;
+  }
+  pc.lap(PHASE_ICM_APPLY);
+  // the last CTA to finish runs the exchange of the round (as k_plain_icm)
+  __shared__ int s_last;
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctl->icm_done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (tid == 0) ctl->icm_done = 0;
+  plain_exchange_body(J, ctl, icm_dE, icm_valid, base, dm);
+}
+
 // Houdayer moves of round ctl->i on thread-block clusters: one cluster of CL
 // CTAs per (chain pair, slot >= lo), each CTA owning the sites of one
 // contiguous colour-order range (on square and cubic lattices a slab of the
@@ -2485,10 +2824,37 @@ static bool plain_launch_icm_cluster(cudaStream_t st, const PtJob& j, const PtJo
   return false;
 }
 
+// The bitmap Houdayer kernel on periodic square and cubic lattices of side 16
+// or 32 (FastInst::lat_L) when its shared memory fits; TAMC_PLAIN_LATTICE=0
+// keeps the site-word kernels (same chain).  Returns false where it does not
+// apply.
+static bool plain_launch_icm_lattice(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl,
+                                     long long* icm_dE, uint32_t* icm_valid, size_t smem_limit,
+                                     unsigned long long* dm) {
+  if (const char* e = getenv("TAMC_PLAIN_LATTICE"))
+    if (e[0] == '0') return false;
+  const uint32_t L = j.F.lat_L, dim = j.F.udeg / 2;
+  if (!L || j.icm_uf || !j.F.fJt || !j.F.fcolt || (dim != 2 && dim != 3)) return false;
+  const size_t smem = std::max(carve_lat(nullptr, nullptr, j.n, j.F.nnz), plain_exch_smem(j.n, j.C, j.ntp));
+  if (smem > smem_limit || j.n / 32 >= 1024) return false;
+  const uint32_t grid = (j.C / 2) * (j.nt - j.lo);
+  auto go = [&](auto k) {
+    TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, dm);
+    TAMC_CUDA(cudaGetLastError());
+  };
+  if (L == 16 && dim == 2) go(k_plain_icm_lat<16, 2>);
+  else if (L == 16 && dim == 3) go(k_plain_icm_lat<16, 3>);
+  else if (L == 32 && dim == 2) go(k_plain_icm_lat<32, 2>);
+  else return false;  // 32^3: the staged couplings do not fit in shared memory
+  return true;
+}
+
 bool plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, PlainCtl* ctl, long long* icm_dE,
                       uint32_t* icm_valid, size_t smem_limit, uint32_t num_sms, unsigned long long* dm) {
   const uint32_t nact = j.nt - j.lo, grid = (j.C / 2) * nact;
   if (!j.icm || grid == 0) return false;
+  if (plain_launch_icm_lattice(st, j, d_job, ctl, icm_dE, icm_valid, smem_limit, dm)) return true;
   if (plain_launch_icm_cluster(st, j, d_job, ctl, icm_dE, icm_valid, smem_limit, num_sms, dm)) return true;
   // as much staging as fits: words and adjacency, words only, nothing
   int stage = j.F.col16 ? 3 : 2;

@@ -37,6 +37,9 @@ FastInst make_fast_inst(const tamc_inst* d) {
   F.col16 = d->d_fcol16;
   F.udeg = d->udeg;
   F.pmj = d->pmj;
+  F.lat_L = d->lat_L;
+  F.fJt = d->d_fJt;
+  F.fcolt = d->d_fcolt;
   F.bias = d->d_fbias;
   F.kd = d->d_fkd;
   F.sus = d->d_fsus;

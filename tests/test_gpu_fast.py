@@ -491,6 +491,38 @@ def test_pt_fast_measurements_match_final_state(tb, po, gpu, monkeypatch, form, 
     assert _rel_ok(np.array([en[-1]]), _f64_energies(po, text, s).reshape(1))
 
 
+@pytest.mark.parametrize("kind", ["2d_L16_pm_C1", "2d_L32_gauss", "3d_L16_gauss_C4", "2d_L12_fallback"])
+def test_plain_lattice_bitmap_houdayer_identical_to_site_words(tb, po, gpu, monkeypatch, kind):
+    """On periodic square and cubic lattices of side 16 or 32 the plain form's
+    Houdayer move runs on site bitmaps in file order (word-parallel growth,
+    couplings staged in shared memory); the chain is the one of the site-word
+    kernel (TAMC_PLAIN_LATTICE=0): states, energies, ground-state log, samples,
+    acceptance and round trips bit for bit.  L = 12 is not a lattice of that
+    kind and takes the site-word kernel either way."""
+    if kind == "2d_L16_pm_C1":
+        text, nt, C, sweeps = gi.lattice(16, 2, "pm", 0), 32, 2, 60
+    elif kind == "2d_L32_gauss":
+        text, nt, C, sweeps = gi.lattice(32, 2, "gauss", 13), 32, 4, 40
+    elif kind == "3d_L16_gauss_C4":
+        text, nt, C, sweeps = gi.lattice(16, 3, "gauss", 0), 64, 2, 30
+    else:
+        text, nt, C, sweeps = gi.lattice(12, 2, "gauss", 14), 24, 2, 40
+    b = po.geometric_betas(0.2, 5.0, nt)
+    p = _pt(tb, sweeps, b, po.lo_beta_idx(b, lo_beta=1.0), C, 8, 5, 7, 0)
+    d = gpu.upload(tb.HostInstance.parse(text))
+    monkeypatch.setenv("TAMC_PT_FORM", "plain")
+    out = []
+    for lat in ("1", "0"):
+        monkeypatch.setenv("TAMC_PLAIN_LATTICE", lat)
+        r = tb.PtRun(d, p, 91).run().sync()
+        ts = r.samples()
+        out.append([*r.state(), *r.gs(), np.array(ts.e), np.array(ts.q), np.array(ts.samples), r.acceptance(),
+                    *r.round_trips()])
+    for a, c in zip(out[0], out[1]):
+        assert np.array_equal(a, c)
+    assert out[0][3].size > 0 and np.any(out[0][-3] > 0)  # a ground-state log and accepted exchanges
+
+
 @pytest.mark.parametrize("kind", ["3d_L8_64", "2d_L32_32", "3d_L16_64_c4"])
 def test_plain_cluster_houdayer_kernel_identical_to_one_cta(tb, po, gpu, monkeypatch, kind):
     """The plain form's Houdayer move on 2- or 4-CTA clusters (sites split over
@@ -507,6 +539,7 @@ def test_plain_cluster_houdayer_kernel_identical_to_one_cta(tb, po, gpu, monkeyp
     p = _pt(tb, sweeps, b, po.lo_beta_idx(b, lo_beta=1.0), C, 8, 5, 7, 0)
     d = gpu.upload(tb.HostInstance.parse(text))
     monkeypatch.setenv("TAMC_PT_FORM", "plain")
+    monkeypatch.setenv("TAMC_PLAIN_LATTICE", "0")  # the site-word kernels on every shape
     out = []
     for cl in ("1", "0"):
         monkeypatch.setenv("TAMC_PLAIN_CLUSTER", cl)
