@@ -23,6 +23,9 @@ struct tamc_pt::FastState {
   tamc::DBuf<uint32_t> ctr;
   uint32_t T = 512;
   size_t smem = 0;
+  // fused runs added to a batch: the random initial replicas are drawn in the
+  // batch's first chunk launch instead of a launch of their own at creation
+  bool init_pending = false;
   // plain form (one instance over the whole GPU)
   bool plain = false;
   tamc::DBuf<tamc::PlainCtl> ctl;
@@ -125,6 +128,8 @@ static float time_tile(tamc_gpu* g, const PtJob& proto, TileChoice t, uint32_t r
 // Set while a server creates runs: every request has its own shape, so the
 // timing autotuner would run per request; the heuristic tile is used instead.
 thread_local bool g_no_autotune = false;
+// Set while a batch adds a run: its initial replicas wait for the first chunk.
+thread_local bool g_defer_init = false;
 
 static TileChoice tune_tile(tamc_gpu* g, const PtJob& j) {
   if (g_no_autotune) return heuristic_tile(g, j);
@@ -419,16 +424,31 @@ void fast_pt_create(tamc_pt* pt, uint64_t seed) {
   pt->fast->job.csr_smem = t.csr;
   pt->fast->smem = fused_smem_bytes(pt->fast->job, t.T, t.csr);
   if (pt->fast->smem > pt->g->smem_optin) fail(TAMC_E_UNSUPPORTED, "instance too large for the fused PT kernel");
+  if (g_defer_init) {  // drawn by the batch's first chunk launch (same chain)
+    pt->fast->init_pending = true;
+    return;
+  }
   launch_one(pt, 0, 0, 1);  // random initial replicas and their energies
 }
 
+// The deferred initial replicas of a batch run, when something reads or runs
+// the run before the batch's first chunk.
+static void ensure_init(tamc_pt* pt) {
+  if (pt->fast && pt->fast->init_pending) {
+    pt->fast->init_pending = false;
+    launch_one(pt, pt->next_sweep, pt->next_sweep, 1);
+  }
+}
+
 void fast_pt_run(tamc_pt* pt, uint32_t sweep_end) {
+  ensure_init(pt);
   const PtCfg& c = pt->cfg;
   while (pt->next_sweep < sweep_end) {
     const uint32_t b = pt->next_sweep;
     const uint32_t e = std::min(sweep_end, b + pt->out.cap);
     if (pt->fast->plain) plain_run_chunk(pt, e - b);
     else launch_one(pt, b, e, 0);
+    pt->out.dirty = true;
     pt->m_next += count_sched(c.sample, c.meas_init, c.num_sweeps, b, e);
     pt->s_next += count_sched(c.sample_states, c.meas_init, c.num_sweeps, b, e);
     pt->next_sweep = e;
@@ -437,6 +457,7 @@ void fast_pt_run(tamc_pt* pt, uint32_t sweep_end) {
 }
 
 void fast_pt_get_state(tamc_pt* pt, int8_t* spins, float* energies) {
+  ensure_init(pt);
   auto* F = pt->fast;
   const PtJob& j = F->job;
   cudaStream_t st = pt->g->stream;
@@ -470,6 +491,7 @@ void fast_pt_set_state(tamc_pt* pt, const int8_t* spins) {
         if (src[perm[s]] < 0) W[(size_t)s * j.nw + o] |= 1u << b;
     }
   TAMC_CUDA(tamc::copy_async(F->W.p, W.data(), W.size() * 4, cudaMemcpyHostToDevice, st));
+  F->init_pending = false;  // the set state replaces the initial replicas
   if (F->plain) plain_init_energies(pt, false);
   else launch_one(pt, pt->next_sweep, pt->next_sweep, 2);  // recompute energies
 }
@@ -530,8 +552,80 @@ struct ChunkRunner {
   cudaEvent_t ev[2] = {nullptr, nullptr};
   double dev_ms = 0.0;
   uint64_t launches = 0;
+  // pinned staging of drain_all
+  char* pin = nullptr;
+  size_t pin_bytes = 0;
+  void pinned(size_t bytes) {
+    if (bytes <= pin_bytes) return;
+    if (pin) cudaFreeHost(pin);
+    pin = nullptr;
+    pin_bytes = 0;
+    TAMC_CUDA(cudaMallocHost((void**)&pin, bytes));
+    pin_bytes = bytes;
+  }
+  // The ground-state logs of every run that ran since its last drain, read in
+  // one pass: the entry counts (asynchronous copies, one synchronisation), then
+  // the entries into pinned staging (one more), instead of two synchronous
+  // reads per run.
+  void drain_all(tamc_gpu* g, const std::vector<tamc_pt*>& jobs) {
+    cudaStream_t st = g->stream;
+    std::vector<tamc_pt*> d;
+    for (auto* pt : jobs)
+      if (pt->out.dirty) d.push_back(pt);
+    if (d.empty()) return;
+    pinned(d.size() * 4);
+    for (size_t k = 0; k < d.size(); ++k)
+      TAMC_CUDA(tamc::copy_async(pin + 4 * k, d[k]->out.gs_count.p, 4, cudaMemcpyDeviceToHost, st));
+    TAMC_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint32_t> cnt(d.size());
+    memcpy(cnt.data(), pin, d.size() * 4);
+    auto up8 = [](size_t x) { return (x + 7) & ~(size_t)7; };
+    size_t bytes = 0;
+    for (size_t k = 0; k < d.size(); ++k) {
+      if (cnt[k] > d[k]->out.cap) fail(TAMC_E_INVAL, "ground-state log overflow");
+      const size_t nw = (d[k]->out.n + 63) / 64;
+      bytes += 2 * up8((size_t)cnt[k] * 4) + (size_t)cnt[k] * nw * 8;
+    }
+    if (bytes) {
+      pinned(bytes);
+      size_t o = 0;
+      for (size_t k = 0; k < d.size(); ++k) {
+        if (!cnt[k]) continue;
+        PtOutputs& out = d[k]->out;
+        const size_t nw = (out.n + 63) / 64;
+        TAMC_CUDA(tamc::copy_async(pin + o, out.gs_steps.p, cnt[k] * 4, cudaMemcpyDeviceToHost, st));
+        o += up8((size_t)cnt[k] * 4);
+        TAMC_CUDA(tamc::copy_async(pin + o, out.gs_E.p, cnt[k] * 4, cudaMemcpyDeviceToHost, st));
+        o += up8((size_t)cnt[k] * 4);
+        TAMC_CUDA(tamc::copy_async(pin + o, out.gs_words.p, cnt[k] * nw * 8, cudaMemcpyDeviceToHost, st));
+        o += (size_t)cnt[k] * nw * 8;
+        TAMC_CUDA(cudaMemsetAsync(out.gs_count.p, 0, 4, st));
+      }
+      TAMC_CUDA(cudaStreamSynchronize(st));
+      o = 0;
+      for (size_t k = 0; k < d.size(); ++k) {
+        if (!cnt[k]) continue;
+        PtOutputs& out = d[k]->out;
+        const size_t nw = (out.n + 63) / 64, b = out.h_steps.size();
+        out.h_steps.resize(b + cnt[k]);
+        out.h_E.resize(b + cnt[k]);
+        out.h_words.resize((b + cnt[k]) * nw);
+        memcpy(out.h_steps.data() + b, pin + o, cnt[k] * 4);
+        o += up8((size_t)cnt[k] * 4);
+        memcpy(out.h_E.data() + b, pin + o, cnt[k] * 4);
+        o += up8((size_t)cnt[k] * 4);
+        memcpy(out.h_words.data() + b * nw, pin + o, cnt[k] * nw * 8);
+        o += (size_t)cnt[k] * nw * 8;
+      }
+    }
+    for (auto* pt : d) {
+      pt->out.pending = 0;
+      pt->out.dirty = false;
+    }
+  }
   ~ChunkRunner() {
     reset();
+    if (pin) cudaFreeHost(pin);
     for (auto e : ev)
       if (e) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -667,7 +761,7 @@ struct ChunkRunner {
     for (uint32_t x = 0; x < na; ++x) {
       tamc_pt* pt = act[x];
       PtJob j = pt->fast->job;
-      j.init = 0;
+      j.init = pt->fast->init_pending ? 1 : 0;  // a batch run's deferred initial replicas
       j.sweep_begin = pt->next_sweep;
       uint32_t rounds = chunk;
       if (balance) {
@@ -743,6 +837,8 @@ struct ChunkRunner {
     for (uint32_t x = 0; x < na; ++x) {
       tamc_pt* pt = act[x];
       const PtCfg& c = pt->cfg;
+      pt->fast->init_pending = false;
+      pt->out.dirty = true;
       pt->m_next += count_sched(c.sample, c.meas_init, c.num_sweeps, pt->next_sweep, ends[x]);
       pt->s_next += count_sched(c.sample_states, c.meas_init, c.num_sweeps, pt->next_sweep, ends[x]);
       pt->next_sweep = ends[x];
@@ -790,7 +886,9 @@ int tamc_gpu_batch_add(tamc_batch* b, tamc_inst* inst, const tamc_pt_params* p, 
   TAMC_API_BEGIN
   if (!b || !inst) fail(TAMC_E_INVAL, "null argument");
   tamc_pt* pt = nullptr;
+  g_defer_init = true;
   const int rc = tamc_gpu_pt_create(inst, p, seed, TAMC_MODE_FAST, &pt);
+  g_defer_init = false;
   if (rc != TAMC_OK) return rc;
   b->jobs.push_back(pt);
   if (job) *job = (uint32_t)(b->jobs.size() - 1);
@@ -807,6 +905,7 @@ int tamc_gpu_batch_run(tamc_batch* b) {
     if (!any) break;
     b->runner.run(b->g, b->jobs, b->chunk, true, false, true);
   }
+  b->runner.drain_all(b->g, b->jobs);
   TAMC_API_END
 }
 

@@ -91,6 +91,7 @@ GsLog PtOutputs::log() const {
 }
 
 void PtOutputs::drain(cudaStream_t st) {
+  if (!dirty) return;  // nothing has run since the last drain: the host copy is current
   uint32_t cnt = 0;
   TAMC_CUDA(tamc::copy_async(&cnt, gs_count.p, 4, cudaMemcpyDeviceToHost, st));
   TAMC_CUDA(cudaStreamSynchronize(st));
@@ -108,6 +109,7 @@ void PtOutputs::drain(cudaStream_t st) {
     TAMC_CUDA(cudaStreamSynchronize(st));
   }
   pending = 0;
+  dirty = false;
 }
 
 static void ref_create(tamc_pt* pt, Xo master) {
@@ -297,6 +299,7 @@ int tamc_gpu_pt_run(tamc_pt* pt, uint32_t sweep_end) {
   if (pt->mode == TAMC_MODE_REF) {
     for (uint32_t i = pt->next_sweep; i < sweep_end; ++i) {
       ref_round(pt, i);
+      pt->out.dirty = true;
       pt->next_sweep = i + 1;
       if (i >= c.meas_init && ++pt->out.pending >= pt->out.cap) {
         check_err(pt);

@@ -65,6 +65,7 @@ struct PtOutputs {
   DBuf<uint64_t> gs_words;
   uint32_t cap = 0;
   uint32_t pending = 0;  // tracked sweeps since the last drain
+  bool dirty = true;     // rounds may have logged entries since the last drain
   std::vector<uint32_t> h_steps;
   std::vector<float> h_E;
   std::vector<uint64_t> h_words;  // concatenated
