@@ -223,6 +223,7 @@ void tamc_gpu_release(tamc_gpu* g) {
   if (g->refs.fetch_sub(1) != 1) return;
   cudaSetDevice(g->device);
   cudaStreamSynchronize(g->stream);
+  runner_pool_release(g);
   cudaFree(g->d_exp);
   cudaStreamDestroy(g->stream);
   dev_cache_release(g->device);

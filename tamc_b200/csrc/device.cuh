@@ -166,6 +166,10 @@ struct tamc_gpu {
 };
 void tamc_gpu_retain(tamc_gpu* g);
 void tamc_gpu_release(tamc_gpu* g);
+namespace tamc {
+// Frees the batch chunk runners kept for reuse on this context.
+void runner_pool_release(tamc_gpu* g);
+}  // namespace tamc
 
 // Reusable device buffers of the host-buffer SA entry point.
 struct SaScratch {

@@ -533,23 +533,65 @@ namespace tamc {
 // launch (jobs ordered longest-remaining-first).  With `graph`, the
 // upload -> reset -> kernel -> readback sequence is captured once per job
 // count / tile and replayed for every later chunk.
+// Ground-state logs of many runs read in one pass: their entry counts, then
+// their entries packed into one staging buffer ([steps][energies][states] per
+// run at 8-byte-aligned offsets), the counts reset.
+struct LogRef {
+  uint32_t* count;
+  const uint32_t* steps;
+  const float* E;
+  const uint64_t* words;
+  uint32_t nw;  // 64-bit words per logged state
+  uint32_t pad;
+};
+__global__ void k_log_counts(const LogRef* __restrict__ r, uint32_t nj, uint32_t* __restrict__ out) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < nj) out[j] = *r[j].count;
+}
+__global__ void k_log_gather(const LogRef* __restrict__ r, const uint32_t* __restrict__ cnt,
+                             const unsigned long long* __restrict__ off, char* __restrict__ stage) {
+  const uint32_t j = blockIdx.x;
+  const LogRef R = r[j];
+  const uint32_t c = cnt[j];
+  char* dst = stage + off[j];
+  const size_t b4 = ((size_t)c * 4 + 7) & ~(size_t)7;
+  for (uint32_t e = threadIdx.x; e < c; e += blockDim.x) {
+    reinterpret_cast<uint32_t*>(dst)[e] = R.steps[e];
+    reinterpret_cast<float*>(dst + b4)[e] = R.E[e];
+  }
+  uint64_t* w = reinterpret_cast<uint64_t*>(dst + 2 * b4);
+  for (size_t x = threadIdx.x; x < (size_t)c * R.nw; x += blockDim.x) w[x] = R.words[x];
+  if (threadIdx.x == 0) *R.count = 0;
+}
+
 struct ChunkRunner {
   DBuf<PtJob> d_jobs;
   DBuf<uint32_t> ctr;
   DBuf<uint32_t> counts;
-  PtJob* h_jobs = nullptr;
-  uint32_t* h_counts = nullptr;
   uint32_t cap_jobs = 0;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  uint32_t g_key[8] = {};  // launch shape of the captured graph
+  // Two buffer sets, so that a batch can enqueue a chunk while the previous
+  // one runs: each has its pinned job table and log counts, its captured
+  // graph and its timing events, and remembers what its chunk advanced.
+  struct Slot {
+    PtJob* h_jobs = nullptr;
+    uint32_t* h_counts = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t key[8] = {};  // launch shape of the captured graph
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool busy = false;
+    std::vector<tamc_pt*> act;
+    uint32_t next = 0;  // the most rounds one run advances per chunk
+    uint64_t seq = 0;   // enqueue order
+  };
+  Slot slots[2];
+  uint64_t seq_next = 0;
   // second stream and fork/join events of the two-class launch
   cudaStream_t aux = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int prio_hi = 0, prio_lo = 0;
   // device time of the chunk launches (CUDA events around each one: the job
-  // table upload, the fused kernel and the count readback) and their number
-  cudaEvent_t ev[2] = {nullptr, nullptr};
+  // table upload, the fused kernels and the count readback) and their number
   double dev_ms = 0.0;
   uint64_t launches = 0;
   // pinned staging of drain_all
@@ -564,58 +606,68 @@ struct ChunkRunner {
     pin_bytes = bytes;
   }
   // The ground-state logs of every run that ran since its last drain, read in
-  // one pass: the entry counts (asynchronous copies, one synchronisation), then
-  // the entries into pinned staging (one more), instead of two synchronous
-  // reads per run.
+  // one pass: a kernel gathers the entry counts (one copy, one
+  // synchronisation), a second packs every log into one staging buffer and
+  // resets the counts (one copy, one more), instead of two synchronous reads
+  // per run.
+  DBuf<LogRef> d_refs;
+  DBuf<uint32_t> d_cnt;
+  DBuf<unsigned long long> d_off;
+  DBuf<char> d_stage;
   void drain_all(tamc_gpu* g, const std::vector<tamc_pt*>& jobs) {
     cudaStream_t st = g->stream;
     std::vector<tamc_pt*> d;
     for (auto* pt : jobs)
       if (pt->out.dirty) d.push_back(pt);
     if (d.empty()) return;
-    pinned(d.size() * 4);
-    for (size_t k = 0; k < d.size(); ++k)
-      TAMC_CUDA(tamc::copy_async(pin + 4 * k, d[k]->out.gs_count.p, 4, cudaMemcpyDeviceToHost, st));
+    const uint32_t nj = (uint32_t)d.size();
+    std::vector<LogRef> refs(nj);
+    for (uint32_t k = 0; k < nj; ++k) {
+      const PtOutputs& o = d[k]->out;
+      refs[k] = LogRef{o.gs_count.p, o.gs_steps.p, o.gs_E.p, o.gs_words.p, (o.n + 63) / 64, 0};
+    }
+    if (d_refs.n < nj) d_refs.alloc(nj);
+    if (d_cnt.n < nj) d_cnt.alloc(nj);
+    if (d_off.n < nj) d_off.alloc(nj);
+    pinned((size_t)nj * 8 + nj * sizeof(LogRef));
+    memcpy(pin, refs.data(), nj * sizeof(LogRef));
+    TAMC_CUDA(tamc::copy_async(d_refs.p, pin, nj * sizeof(LogRef), cudaMemcpyHostToDevice, st));
+    k_log_counts<<<(nj + 255) / 256, 256, 0, st>>>(d_refs.p, nj, d_cnt.p);
+    TAMC_CUDA(cudaGetLastError());
+    g->count();
+    uint32_t* cnt_h = reinterpret_cast<uint32_t*>(pin + nj * sizeof(LogRef));
+    TAMC_CUDA(tamc::copy_async(cnt_h, d_cnt.p, nj * 4, cudaMemcpyDeviceToHost, st));
     TAMC_CUDA(cudaStreamSynchronize(st));
-    std::vector<uint32_t> cnt(d.size());
-    memcpy(cnt.data(), pin, d.size() * 4);
+    std::vector<uint32_t> cnt(cnt_h, cnt_h + nj);
     auto up8 = [](size_t x) { return (x + 7) & ~(size_t)7; };
+    std::vector<unsigned long long> off(nj);
     size_t bytes = 0;
-    for (size_t k = 0; k < d.size(); ++k) {
+    for (uint32_t k = 0; k < nj; ++k) {
       if (cnt[k] > d[k]->out.cap) fail(TAMC_E_INVAL, "ground-state log overflow");
-      const size_t nw = (d[k]->out.n + 63) / 64;
-      bytes += 2 * up8((size_t)cnt[k] * 4) + (size_t)cnt[k] * nw * 8;
+      off[k] = bytes;
+      bytes += 2 * up8((size_t)cnt[k] * 4) + (size_t)cnt[k] * refs[k].nw * 8;
     }
     if (bytes) {
-      pinned(bytes);
-      size_t o = 0;
-      for (size_t k = 0; k < d.size(); ++k) {
-        if (!cnt[k]) continue;
-        PtOutputs& out = d[k]->out;
-        const size_t nw = (out.n + 63) / 64;
-        TAMC_CUDA(tamc::copy_async(pin + o, out.gs_steps.p, cnt[k] * 4, cudaMemcpyDeviceToHost, st));
-        o += up8((size_t)cnt[k] * 4);
-        TAMC_CUDA(tamc::copy_async(pin + o, out.gs_E.p, cnt[k] * 4, cudaMemcpyDeviceToHost, st));
-        o += up8((size_t)cnt[k] * 4);
-        TAMC_CUDA(tamc::copy_async(pin + o, out.gs_words.p, cnt[k] * nw * 8, cudaMemcpyDeviceToHost, st));
-        o += (size_t)cnt[k] * nw * 8;
-        TAMC_CUDA(cudaMemsetAsync(out.gs_count.p, 0, 4, st));
-      }
+      if (d_stage.n < bytes) d_stage.alloc(bytes);
+      pinned(std::max(bytes, (size_t)nj * 8));
+      memcpy(pin, off.data(), nj * 8);
+      TAMC_CUDA(tamc::copy_async(d_off.p, pin, nj * 8, cudaMemcpyHostToDevice, st));
+      k_log_gather<<<nj, 128, 0, st>>>(d_refs.p, d_cnt.p, d_off.p, d_stage.p);
+      TAMC_CUDA(cudaGetLastError());
+      g->count();
+      TAMC_CUDA(tamc::copy_async(pin, d_stage.p, bytes, cudaMemcpyDeviceToHost, st));
       TAMC_CUDA(cudaStreamSynchronize(st));
-      o = 0;
-      for (size_t k = 0; k < d.size(); ++k) {
+      for (uint32_t k = 0; k < nj; ++k) {
         if (!cnt[k]) continue;
         PtOutputs& out = d[k]->out;
-        const size_t nw = (out.n + 63) / 64, b = out.h_steps.size();
+        const size_t nw = refs[k].nw, b = out.h_steps.size();
+        const char* src = pin + off[k];
         out.h_steps.resize(b + cnt[k]);
         out.h_E.resize(b + cnt[k]);
         out.h_words.resize((b + cnt[k]) * nw);
-        memcpy(out.h_steps.data() + b, pin + o, cnt[k] * 4);
-        o += up8((size_t)cnt[k] * 4);
-        memcpy(out.h_E.data() + b, pin + o, cnt[k] * 4);
-        o += up8((size_t)cnt[k] * 4);
-        memcpy(out.h_words.data() + b * nw, pin + o, cnt[k] * nw * 8);
-        o += (size_t)cnt[k] * nw * 8;
+        memcpy(out.h_steps.data() + b, src, cnt[k] * 4);
+        memcpy(out.h_E.data() + b, src + up8((size_t)cnt[k] * 4), cnt[k] * 4);
+        memcpy(out.h_words.data() + b * nw, src + 2 * up8((size_t)cnt[k] * 4), cnt[k] * nw * 8);
       }
     }
     for (auto* pt : d) {
@@ -626,31 +678,37 @@ struct ChunkRunner {
   ~ChunkRunner() {
     reset();
     if (pin) cudaFreeHost(pin);
-    for (auto e : ev)
-      if (e) cudaEventDestroy(e);
+    for (auto& sl : slots)
+      for (auto e : sl.ev)
+        if (e) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
     if (aux) cudaStreamDestroy(aux);
   }
   void reset() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    exec = nullptr;
-    graph = nullptr;
-    if (h_jobs) cudaFreeHost(h_jobs);
-    if (h_counts) cudaFreeHost(h_counts);
-    h_jobs = nullptr;
-    h_counts = nullptr;
+    for (auto& sl : slots) {
+      if (sl.exec) cudaGraphExecDestroy(sl.exec);
+      if (sl.graph) cudaGraphDestroy(sl.graph);
+      sl.exec = nullptr;
+      sl.graph = nullptr;
+      if (sl.h_jobs) cudaFreeHost(sl.h_jobs);
+      if (sl.h_counts) cudaFreeHost(sl.h_counts);
+      sl.h_jobs = nullptr;
+      sl.h_counts = nullptr;
+      sl.busy = false;
+    }
     cap_jobs = 0;
   }
   void reserve(uint32_t n) {
     if (n <= cap_jobs) return;
     reset();
     cap_jobs = std::max(n, 16u);
-    for (auto& e : ev)
-      if (!e) TAMC_CUDA(cudaEventCreate(&e));
-    TAMC_CUDA(cudaMallocHost((void**)&h_jobs, cap_jobs * sizeof(PtJob)));
-    TAMC_CUDA(cudaMallocHost((void**)&h_counts, cap_jobs * sizeof(uint32_t)));
+    for (auto& sl : slots) {
+      for (auto& e : sl.ev)
+        if (!e) TAMC_CUDA(cudaEventCreate(&e));
+      TAMC_CUDA(cudaMallocHost((void**)&sl.h_jobs, cap_jobs * sizeof(PtJob)));
+      TAMC_CUDA(cudaMallocHost((void**)&sl.h_counts, cap_jobs * sizeof(uint32_t)));
+    }
     d_jobs.alloc(cap_jobs);
     ctr.alloc(2);
     counts.alloc(cap_jobs);
@@ -704,13 +762,15 @@ struct ChunkRunner {
   // priority, one CTA per SM, and the small runs' launch beside it with two or
   // more CTAs per SM, so that small runs no longer hold a whole SM each after
   // the large ones have taken theirs (TAMC_PT_SPLIT=0: one launch).
-  void run(tamc_gpu* g, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance = false,
-           bool lazy_logs = false) {
+  // Enqueues one chunk into slot `sl` (which must not be busy) and returns
+  // without waiting; the runs' host-side progress is advanced at once.
+  // Returns false when no run has rounds left.
+  bool enqueue(tamc_gpu* g, Slot& sl, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance) {
     cudaStream_t st = g->stream;
     act.erase(std::remove_if(act.begin(), act.end(),
                              [](tamc_pt* p) { return p->next_sweep >= p->cfg.num_sweeps; }),
               act.end());
-    if (act.empty()) return;
+    if (act.empty()) return false;
     auto remaining = [](const tamc_pt* p) {
       return (uint64_t)(p->cfg.num_sweeps - p->next_sweep) * (p->fast->job.cost / std::max(1u, p->cfg.num_sweeps));
     };
@@ -754,7 +814,11 @@ struct ChunkRunner {
       A = shape(g, act, T);
     }
     const uint32_t na = (uint32_t)act.size();
-    reserve(na);
+    if (na > cap_jobs) {  // growing the buffers: nothing may be in flight
+      finish_all(g, false, chunk);
+      reserve(na);
+    }
+    PtJob* const h_jobs = sl.h_jobs;
     std::vector<uint32_t> ends(na);
     double c_max = 1.0;  // the largest cost of one round among the runs
     for (auto* pt : act) c_max = std::max(c_max, (double)pt->fast->job.cost / std::max(1u, pt->cfg.num_sweeps));
@@ -775,6 +839,7 @@ struct ChunkRunner {
       j.count_out = counts.p + x;
       h_jobs[x] = j;
     }
+    sl.next = balance ? 8 * chunk : chunk;
     if (split && !aux) {
       int least = 0, greatest = 0;
       TAMC_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -800,40 +865,35 @@ struct ChunkRunner {
     };
     if (use_graph) {
       const uint32_t key[8] = {na, nb, A.grid, A.T, (uint32_t)A.smem, B.grid, B.T, (uint32_t)B.smem};
-      if (!exec || memcmp(key, g_key, sizeof(key)) != 0) {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
+      if (!sl.exec || memcmp(key, sl.key, sizeof(key)) != 0) {
+        if (sl.exec) cudaGraphExecDestroy(sl.exec);
+        if (sl.graph) cudaGraphDestroy(sl.graph);
+        sl.exec = nullptr;
+        sl.graph = nullptr;
         TAMC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         // the graph's two copies are counted at every replay below
         cudaMemcpyAsync(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st);
         cudaMemsetAsync(ctr.p, 0, 8, st);
         launch_all();
-        cudaMemcpyAsync(h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st);
-        TAMC_CUDA(cudaStreamEndCapture(st, &graph));
-        TAMC_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        memcpy(g_key, key, sizeof(key));
+        cudaMemcpyAsync(sl.h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st);
+        TAMC_CUDA(cudaStreamEndCapture(st, &sl.graph));
+        TAMC_CUDA(cudaGraphInstantiate(&sl.exec, sl.graph, 0));
+        memcpy(sl.key, key, sizeof(key));
       }
-      TAMC_CUDA(cudaEventRecord(ev[0], st));
-      TAMC_CUDA(cudaGraphLaunch(exec, st));
-      TAMC_CUDA(cudaEventRecord(ev[1], st));
+      TAMC_CUDA(cudaEventRecord(sl.ev[0], st));
+      TAMC_CUDA(cudaGraphLaunch(sl.exec, st));
+      TAMC_CUDA(cudaEventRecord(sl.ev[1], st));
       count_copy(na * sizeof(PtJob), cudaMemcpyHostToDevice);
       count_copy(na * 4, cudaMemcpyDeviceToHost);
     } else {
-      TAMC_CUDA(cudaEventRecord(ev[0], st));
+      TAMC_CUDA(cudaEventRecord(sl.ev[0], st));
       TAMC_CUDA(tamc::copy_async(d_jobs.p, h_jobs, na * sizeof(PtJob), cudaMemcpyHostToDevice, st));
       TAMC_CUDA(cudaMemsetAsync(ctr.p, 0, 8, st));
       launch_all();
-      TAMC_CUDA(tamc::copy_async(h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st));
-      TAMC_CUDA(cudaEventRecord(ev[1], st));
+      TAMC_CUDA(tamc::copy_async(sl.h_counts, counts.p, na * 4, cudaMemcpyDeviceToHost, st));
+      TAMC_CUDA(cudaEventRecord(sl.ev[1], st));
     }
     g->count(split ? 2 : 1);
-    TAMC_CUDA(cudaStreamSynchronize(st));
-    float ms = 0.0f;
-    TAMC_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-    dev_ms += ms;
-    ++launches;
     for (uint32_t x = 0; x < na; ++x) {
       tamc_pt* pt = act[x];
       const PtCfg& c = pt->cfg;
@@ -842,10 +902,59 @@ struct ChunkRunner {
       pt->m_next += count_sched(c.sample, c.meas_init, c.num_sweeps, pt->next_sweep, ends[x]);
       pt->s_next += count_sched(c.sample_states, c.meas_init, c.num_sweeps, pt->next_sweep, ends[x]);
       pt->next_sweep = ends[x];
-      const uint32_t next = std::min(pt->out.cap, balance ? 8 * chunk : chunk);
-      if (h_counts[x] && (!lazy_logs || h_counts[x] + next > pt->out.cap)) pt->out.drain(st);
-      else if (!h_counts[x]) pt->out.pending = 0;
     }
+    sl.act = std::move(act);
+    sl.busy = true;
+    sl.seq = seq_next++;
+    return true;
+  }
+
+  // Waits for slot `sl`'s chunk, adds its device time and reads its log
+  // counts.  `lazy`: a log is drained only when the entries it may hold after
+  // the next `ahead` chunks (at most `next` rounds each, one entry per round)
+  // could exceed its capacity; otherwise every non-empty log is drained.
+  void finish(tamc_gpu* g, Slot& sl, bool lazy, uint32_t ahead) {
+    if (!sl.busy) return;
+    sl.busy = false;
+    TAMC_CUDA(cudaEventSynchronize(sl.ev[1]));
+    float ms = 0.0f;
+    TAMC_CUDA(cudaEventElapsedTime(&ms, sl.ev[0], sl.ev[1]));
+    dev_ms += ms;
+    ++launches;
+    for (size_t x = 0; x < sl.act.size(); ++x) {
+      tamc_pt* pt = sl.act[x];
+      const uint32_t cnt = sl.h_counts[x];
+      const uint64_t next = std::min<uint64_t>(pt->out.cap, sl.next);
+      if (cnt && (!lazy || cnt + ahead * next > pt->out.cap)) pt->out.drain(g->stream);
+      else if (!cnt) pt->out.pending = 0;
+    }
+  }
+  void finish_all(tamc_gpu* g, bool lazy, uint32_t) {
+    Slot* a = &slots[0];
+    Slot* b = &slots[1];
+    if (b->busy && (!a->busy || b->seq < a->seq)) std::swap(a, b);  // the older chunk first
+    finish(g, *a, lazy, 1);
+    finish(g, *b, lazy, 1);
+  }
+
+  // Advances every run in `act` by up to `chunk` rounds (one chunk) and waits.
+  void run(tamc_gpu* g, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance = false,
+           bool lazy_logs = false) {
+    if (enqueue(g, slots[0], std::move(act), chunk, use_graph, balance)) finish(g, slots[0], lazy_logs, 1);
+  }
+
+  // Runs every run in `jobs` to its end, chunk after chunk, with the next
+  // chunk enqueued before the previous one has finished (two buffer sets, so
+  // no host gap between chunks); the logs are drained lazily, looking two
+  // chunks ahead, and once at the end.
+  void run_all(tamc_gpu* g, const std::vector<tamc_pt*>& jobs, uint32_t chunk) {
+    uint32_t k = 0;
+    for (;; k ^= 1) {
+      Slot& sl = slots[k];
+      finish(g, sl, true, 2);  // the chunk that used these buffers two chunks ago
+      if (!enqueue(g, sl, jobs, chunk, true, false)) break;
+    }
+    finish_all(g, true, chunk);
   }
 };
 
@@ -859,14 +968,51 @@ void chunk_runner_free(ChunkRunner* r) { delete r; }
 
 using namespace tamc;
 
+namespace tamc {
+// Chunk runners kept per context after their batch is destroyed, with their
+// buffers and captured graphs, so that the next batch of the same shape
+// replays them instead of capturing anew.
+static std::mutex g_pool_mu;
+static std::map<tamc_gpu*, std::vector<ChunkRunner*>> g_pool;
+static ChunkRunner* runner_take(tamc_gpu* g) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto& v = g_pool[g];
+  if (v.empty()) return new ChunkRunner();
+  ChunkRunner* r = v.back();
+  v.pop_back();
+  return r;
+}
+static void runner_give(tamc_gpu* g, ChunkRunner* r) {
+  for (auto& sl : r->slots) sl.busy = false;
+  r->dev_ms = 0.0;
+  r->launches = 0;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  auto& v = g_pool[g];
+  if (v.size() >= 4) delete r;
+  else v.push_back(r);
+}
+void runner_pool_release(tamc_gpu* g) {
+  std::vector<ChunkRunner*> v;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pool.find(g);
+    if (it == g_pool.end()) return;
+    v.swap(it->second);
+    g_pool.erase(it);
+  }
+  for (auto* r : v) delete r;
+}
+}  // namespace tamc
+
 struct tamc_batch {
   tamc_gpu* g = nullptr;
   std::vector<tamc_pt*> jobs;
-  ChunkRunner runner;
+  ChunkRunner* runner = nullptr;
   uint32_t chunk = 256;
+  bool logs_pending = false;  // the last run's ground-state logs are still on the device
   ~tamc_batch() {
-    runner.reset();
     for (auto* p : jobs) tamc_gpu_pt_destroy(p);
+    if (runner) runner_give(g, runner);
   }
 };
 
@@ -877,6 +1023,7 @@ int tamc_gpu_batch_create(tamc_gpu* g, tamc_batch** out) {
   if (!g || !out) fail(TAMC_E_INVAL, "null argument");
   auto* b = new tamc_batch();
   b->g = g;
+  b->runner = runner_take(g);
   tamc_gpu_retain(g);
   *out = b;
   TAMC_API_END
@@ -899,13 +1046,8 @@ int tamc_gpu_batch_run(tamc_batch* b) {
   TAMC_API_BEGIN
   if (!b) fail(TAMC_E_INVAL, "null batch");
   TAMC_CUDA(cudaSetDevice(b->g->device));
-  for (;;) {
-    bool any = false;
-    for (auto* pt : b->jobs) any |= pt->next_sweep < pt->cfg.num_sweeps;
-    if (!any) break;
-    b->runner.run(b->g, b->jobs, b->chunk, true, false, true);
-  }
-  b->runner.drain_all(b->g, b->jobs);
+  b->runner->run_all(b->g, b->jobs, b->chunk);
+  b->logs_pending = true;  // drained, all runs at once, by the first log read
   TAMC_API_END
 }
 
@@ -945,7 +1087,13 @@ int tamc_gpu_batch_acceptance(tamc_batch* b, uint32_t job, uint32_t* counts) {
 int tamc_gpu_batch_gs(tamc_batch* b, uint32_t job, uint32_t cap, uint32_t* count, uint32_t* steps, float* energies,
                       uint64_t* states) {
   TAMC_API_BEGIN
-  return tamc_gpu_pt_gs(job_of(b, job), cap, count, steps, energies, states);
+  tamc_pt* pt = job_of(b, job);
+  if (b->logs_pending) {
+    TAMC_CUDA(cudaSetDevice(b->g->device));
+    b->runner->drain_all(b->g, b->jobs);
+    b->logs_pending = false;
+  }
+  return tamc_gpu_pt_gs(pt, cap, count, steps, energies, states);
   TAMC_API_END
 }
 int tamc_gpu_batch_samples_dims(tamc_batch* b, uint32_t job, uint32_t* M, uint32_t* S, uint32_t* Z, uint32_t* nchi) {
@@ -961,8 +1109,8 @@ int tamc_gpu_batch_samples(tamc_batch* b, uint32_t job, float* e, int32_t* q, fl
 int tamc_gpu_batch_device_time(tamc_batch* b, double* ms, uint64_t* launches) {
   TAMC_API_BEGIN
   if (!b) fail(TAMC_E_INVAL, "null batch");
-  if (ms) *ms = b->runner.dev_ms;
-  if (launches) *launches = b->runner.launches;
+  if (ms) *ms = b->runner->dev_ms;
+  if (launches) *launches = b->runner->launches;
   TAMC_API_END
 }
 int tamc_gpu_batch_tile(tamc_batch* b, uint32_t job, uint32_t* cta_threads, uint32_t* slots_per_task, int32_t* csr_in_smem) {
