@@ -310,6 +310,45 @@ def test_batch_two_class_launch_identical_to_one_launch(tb, po, gpu, monkeypatch
         assert all(np.array_equal(np.asarray(x), np.asarray(y)) for x, y in zip(t1, t0))
 
 
+def test_batch_reuse_and_deferred_initial_state(tb, po, gpu):
+    """A batch's runs draw their initial replicas in the first chunk launch; read
+    before any run, a batch run's state is a standalone run's initial state.  A
+    second batch of the same runs reuses the first one's chunk runner (buffers
+    and captured graphs kept per context) and gives the same results, and a
+    batch of another shape in between does not disturb it."""
+    jobs = _mixed_jobs(po, 5, 3)
+
+    def make():
+        b = tb.Batch(gpu)
+        for k, (text, bb, lo) in enumerate(jobs):
+            d = gpu.upload(tb.HostInstance.parse(text))
+            b.add(d, tb.PtParams(90 + 10 * k, bb, lo, 0.5, True, 2, 4, 6, None, 0), 500 + k)
+        return b
+
+    b0 = make()
+    text, bb, lo = jobs[0]
+    alone = tb.PtRun(gpu.upload(tb.HostInstance.parse(text)), tb.PtParams(90, bb, lo, 0.5, True, 2, 4, 6, None, 0),
+                     500)
+    S0, E0 = b0.state(0)  # before the batch has run
+    Sa, Ea = alone.state()
+    assert np.array_equal(S0, Sa) and np.array_equal(E0, Ea)
+    b0.run()
+    first = [(b0.state(k), b0.gs(k)[1], b0.acceptance(k)) for k in range(len(jobs))]
+    del b0
+    other = tb.Batch(gpu)  # another shape on the pooled runner
+    d = gpu.upload(tb.HostInstance.parse(gi.lattice(8, 2, "gauss", 1)))
+    other.add(d, tb.PtParams(40, po.geometric_betas(0.2, 5.0, 8), 4, 0.5, True, 2, 4), 1)
+    other.run()
+    del other
+    b1 = make()
+    b1.run()
+    for k in range(len(jobs)):
+        (S, E), g, a = first[k]
+        S1, E1 = b1.state(k)
+        assert np.array_equal(S, S1) and np.array_equal(E, E1), k
+        assert np.array_equal(g, b1.gs(k)[1]) and np.array_equal(a, b1.acceptance(k))
+
+
 def test_server_results_same_alone_and_in_the_mix(tb, po, gpu):
     jobs = _mixed_jobs(po, 7, 1)
     srv = tb.Server(gpu, hbm_budget_bytes=1 << 30, max_active=3, chunk_sweeps=40)
