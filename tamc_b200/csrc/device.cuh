@@ -65,6 +65,19 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
   return c;
 }
 
+// The same generator with each round's two products as 32x32->64 multiplies
+// (one wide multiply each instead of a low and a high one): the same outputs.
+__device__ __forceinline__ uint4 philox4x32_10w(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c.x, p1 = (uint64_t)0xCD9E8D57u * c.z;
+    c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k.x, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k.y, (uint32_t)p0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
 // The same generator with the ten round keys computed once (they depend only
 // on the seed): saves the two key additions per round in hot loops, and each
 // multiply is one 32x32->64 product (a wide multiply instead of separate lo

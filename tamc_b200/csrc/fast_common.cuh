@@ -278,7 +278,7 @@ __device__ __forceinline__ uint32_t msc_flip(const MscLevels& L, const uint32_t*
   }
   uint32_t lt = 0;
   for (uint32_t kk = 0; kk < 8 && und; ++kk)
-    msc_step4<DEG>(philox4x32_10(make_uint4(s, i, (wo << 8) | kk, PTAG_MSC), key), pl, L, kk, und, lt);
+    msc_step4<DEG>(philox4x32_10w(make_uint4(s, i, (wo << 8) | kk, PTAG_MSC), key), pl, L, kk, und, lt);
   return ~uphill | always | lt;
 }
 
@@ -303,8 +303,8 @@ __device__ __forceinline__ void msc_flip2(const MscLevels& L0, const MscLevels& 
   }
   uint32_t lt0 = 0, lt1 = 0;
   for (uint32_t kk = 0; kk < 8 && (und0 | und1); ++kk) {
-    const uint4 r0 = philox4x32_10(make_uint4(s, i, (wo << 8) | kk, PTAG_MSC), key);
-    const uint4 r1 = philox4x32_10(make_uint4(s, i, ((wo + 1) << 8) | kk, PTAG_MSC), key);
+    const uint4 r0 = philox4x32_10w(make_uint4(s, i, (wo << 8) | kk, PTAG_MSC), key);
+    const uint4 r1 = philox4x32_10w(make_uint4(s, i, ((wo + 1) << 8) | kk, PTAG_MSC), key);
     msc_step4<DEG>(r0, pl0, L0, kk, und0, lt0);
     msc_step4<DEG>(r1, pl1, L1, kk, und1, lt1);
   }

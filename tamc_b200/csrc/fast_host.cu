@@ -765,7 +765,8 @@ struct ChunkRunner {
   // Enqueues one chunk into slot `sl` (which must not be busy) and returns
   // without waiting; the runs' host-side progress is advanced at once.
   // Returns false when no run has rounds left.
-  bool enqueue(tamc_gpu* g, Slot& sl, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance) {
+  bool enqueue(tamc_gpu* g, Slot& sl, std::vector<tamc_pt*> act, uint32_t chunk, bool use_graph, bool balance,
+               bool by_size = false) {
     cudaStream_t st = g->stream;
     act.erase(std::remove_if(act.begin(), act.end(),
                              [](tamc_pt* p) { return p->next_sweep >= p->cfg.num_sweeps; }),
@@ -787,7 +788,11 @@ struct ChunkRunner {
       // run alone on an otherwise idle SM
       std::vector<tamc_pt*> big, small;
       uint32_t Ts = 128;
-      for (auto* pt : act) (pt->fast->T >= 512 ? big : small).push_back(pt);
+      // (`by_size`: runs of at most 512 sites also go to the small class
+      // whatever their tile, so that a batch built with heuristic tiles, all
+      // of 512 threads, still splits)
+      for (auto* pt : act)
+        (pt->fast->T >= 512 && !(by_size && pt->fast->job.n <= 512) ? big : small).push_back(pt);
       if (const char* e = getenv("TAMC_PT_TSMALL")) {  // the small class's CTA size, for measurements
         const int t = atoi(e);
         if (t == 128 || t == 256) Ts = (uint32_t)t;
@@ -952,7 +957,7 @@ struct ChunkRunner {
     for (;; k ^= 1) {
       Slot& sl = slots[k];
       finish(g, sl, true, 2);  // the chunk that used these buffers two chunks ago
-      if (!enqueue(g, sl, jobs, chunk, true, false)) break;
+      if (!enqueue(g, sl, jobs, chunk, true, false, true)) break;
     }
     finish_all(g, true, chunk);
   }
