@@ -1015,9 +1015,41 @@ struct tamc_batch {
   ChunkRunner* runner = nullptr;
   uint32_t chunk = 256;
   bool logs_pending = false;  // the last run's ground-state logs are still on the device
+  // acceptance counts of every run, read in one pass on the first request
+  // after a run (asynchronous copies into pinned memory, one synchronisation)
+  bool acc_pending = true;
+  std::vector<std::vector<uint32_t>> acc;
+  uint32_t* acc_pin = nullptr;
+  size_t acc_pin_n = 0;
   ~tamc_batch() {
     for (auto* p : jobs) tamc_gpu_pt_destroy(p);
     if (runner) runner_give(g, runner);
+    if (acc_pin) cudaFreeHost(acc_pin);
+  }
+  void read_acceptance() {
+    size_t total = 0;
+    for (auto* pt : jobs) total += pt->fast->acc.n;
+    if (total > acc_pin_n) {
+      if (acc_pin) cudaFreeHost(acc_pin);
+      acc_pin = nullptr;
+      acc_pin_n = 0;
+      TAMC_CUDA(cudaMallocHost((void**)&acc_pin, std::max<size_t>(total, 1) * 4));
+      acc_pin_n = total;
+    }
+    size_t o = 0;
+    for (auto* pt : jobs) {
+      TAMC_CUDA(tamc::copy_async(acc_pin + o, pt->fast->acc.p, pt->fast->acc.n * 4, cudaMemcpyDeviceToHost,
+                                 g->stream));
+      o += pt->fast->acc.n;
+    }
+    TAMC_CUDA(cudaStreamSynchronize(g->stream));
+    acc.resize(jobs.size());
+    o = 0;
+    for (size_t k = 0; k < jobs.size(); ++k) {
+      acc[k].assign(acc_pin + o, acc_pin + o + jobs[k]->fast->acc.n);
+      o += jobs[k]->fast->acc.n;
+    }
+    acc_pending = false;
   }
 };
 
@@ -1043,6 +1075,7 @@ int tamc_gpu_batch_add(tamc_batch* b, tamc_inst* inst, const tamc_pt_params* p, 
   g_defer_init = false;
   if (rc != TAMC_OK) return rc;
   b->jobs.push_back(pt);
+  b->acc_pending = true;
   if (job) *job = (uint32_t)(b->jobs.size() - 1);
   TAMC_API_END
 }
@@ -1053,6 +1086,7 @@ int tamc_gpu_batch_run(tamc_batch* b) {
   TAMC_CUDA(cudaSetDevice(b->g->device));
   b->runner->run_all(b->g, b->jobs, b->chunk);
   b->logs_pending = true;  // drained, all runs at once, by the first log read
+  b->acc_pending = true;
   TAMC_API_END
 }
 
@@ -1086,7 +1120,18 @@ int tamc_gpu_batch_round_trips(tamc_batch* b, uint32_t job, uint8_t* tags, uint3
 }
 int tamc_gpu_batch_acceptance(tamc_batch* b, uint32_t job, uint32_t* counts) {
   TAMC_API_BEGIN
-  return tamc_gpu_pt_acceptance(job_of(b, job), counts);
+  tamc_pt* pt = job_of(b, job);
+  if (!counts) fail(TAMC_E_INVAL, "null argument");
+  if (!pt->fast || pt->fast->plain) return tamc_gpu_pt_acceptance(pt, counts);
+  TAMC_CUDA(cudaSetDevice(b->g->device));
+  if (b->acc_pending) b->read_acceptance();
+  const PtCfg& c = pt->cfg;
+  const std::vector<uint32_t>& a = b->acc[job];  // [C][nt]
+  for (uint32_t t = 0; t < c.nt; ++t) {
+    uint32_t s = 0;
+    for (uint32_t ch = 0; ch < c.C; ++ch) s += a[(size_t)ch * c.nt + t];
+    counts[t] = s;
+  }
   TAMC_API_END
 }
 int tamc_gpu_batch_gs(tamc_batch* b, uint32_t job, uint32_t cap, uint32_t* count, uint32_t* steps, float* energies,
