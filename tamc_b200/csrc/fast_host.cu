@@ -820,7 +820,7 @@ struct ChunkRunner {
     }
     const uint32_t na = (uint32_t)act.size();
     if (na > cap_jobs) {  // growing the buffers: nothing may be in flight
-      finish_all(g, false, chunk);
+      finish_all(g, false);
       reserve(na);
     }
     PtJob* const h_jobs = sl.h_jobs;
@@ -934,7 +934,7 @@ struct ChunkRunner {
       else if (!cnt) pt->out.pending = 0;
     }
   }
-  void finish_all(tamc_gpu* g, bool lazy, uint32_t) {
+  void finish_all(tamc_gpu* g, bool lazy) {
     Slot* a = &slots[0];
     Slot* b = &slots[1];
     if (b->busy && (!a->busy || b->seq < a->seq)) std::swap(a, b);  // the older chunk first
@@ -959,7 +959,7 @@ struct ChunkRunner {
       finish(g, sl, true, 2);  // the chunk that used these buffers two chunks ago
       if (!enqueue(g, sl, jobs, chunk, true, false, true)) break;
     }
-    finish_all(g, true, chunk);
+    finish_all(g, true);
   }
 };
 
