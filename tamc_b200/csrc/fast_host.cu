@@ -278,6 +278,8 @@ static void launch_one(tamc_pt* pt, uint32_t begin, uint32_t end, int init) {
 }
 
 // ---- plain form: one launch per sweep phase over the whole GPU
+// (the head launch of a round without measurements returns at once; leaving
+// it out of the captured chunk measured slower on C4, so every round has one)
 static void plain_enqueue_rounds(tamc_pt* pt, uint32_t K) {
   auto* F = pt->fast;
   const PtJob& j = F->job;

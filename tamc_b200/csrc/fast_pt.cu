@@ -1006,21 +1006,50 @@ __device__ void exchange_decide(const PtJob& J, Smem& S, uint32_t i) {
       }
       D = (uint64_t)__ballot_sync(0xffffffffu, d[0]) | ((uint64_t)__ballot_sync(0xffffffffu, d[1]) << 32);
     } else {
-      if (lane == 0) {
-        float carry = 0.0f;
-        bool prev = false;
-        for (uint32_t j = 0; j + 1 < nt; ++j) {
-          float des = (float)Ec[j + 1] - (float)Ec[j];
-          if (prev) des += carry;  // ΔE propagation after a swap (tamc-core/src/pt.rs:138-141)
-          const float dlt = (S.xb ? XS.dbeta[j] : J.betas[j + 1] - J.betas[j]) * des;
-          const bool dj = dlt >= 0.0f ||
-                          u24(philox4x32_10(make_uint4(j, i, c, PTAG_EXCH), J.key).x) < __expf(dlt);
-          if (dj) D |= 1ull << j;
-          prev = dj;
-          carry = des;
+      // Serial semantics: pair j sees ΔE_j plus the carried ΔE_{j-1} when pair
+      // j - 1 swapped (tamc-core/src/pt.rs:138-141).  The draws, Δβ, ΔE_j and
+      // the decisions without a carry do not depend on earlier pairs, so lane
+      // j % 32 computes them for pair j in parallel; the walk over the pairs
+      // then redoes only the decisions whose lower pair swapped, with the same
+      // float operations as a plain sequential loop (same decisions).
+      float des0[2], db[2], u[2];
+      bool d0[2];
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t j = lane + 32u * h;
+        des0[h] = 0.0f;
+        db[h] = 0.0f;
+        u[h] = 1.0f;
+        d0[h] = false;
+        if (j + 1 < nt) {
+          des0[h] = (float)Ec[j + 1] - (float)Ec[j];
+          db[h] = S.xb ? XS.dbeta[j] : J.betas[j + 1] - J.betas[j];
+          u[h] = u24(philox4x32_10(make_uint4(j, i, c, PTAG_EXCH), J.key).x);
+          const float dlt = db[h] * des0[h];
+          d0[h] = dlt >= 0.0f || u[h] < __expf(dlt);
         }
       }
-      D = __shfl_sync(0xffffffffu, D, 0);
+      const uint64_t D0 =
+          (uint64_t)__ballot_sync(0xffffffffu, d0[0]) | ((uint64_t)__ballot_sync(0xffffffffu, d0[1]) << 32);
+      float carry = 0.0f;
+      bool prev = false;
+      for (uint32_t j = 0; j + 1 < nt; ++j) {  // warp-uniform: every lane walks the same values
+        const bool hi = j >= 32u;
+        const float e = __shfl_sync(0xffffffffu, hi ? des0[1] : des0[0], j & 31u);
+        const float b = __shfl_sync(0xffffffffu, hi ? db[1] : db[0], j & 31u);
+        const float uj = __shfl_sync(0xffffffffu, hi ? u[1] : u[0], j & 31u);
+        float des = e;
+        bool dj;
+        if (prev) {
+          des = e + carry;
+          const float dlt = b * des;
+          dj = dlt >= 0.0f || uj < __expf(dlt);
+        } else {
+          dj = (D0 >> j) & 1ull;
+        }
+        if (dj) D |= 1ull << j;
+        prev = dj;
+        carry = des;
+      }
     }
     // acceptance counts, slot permutation of energies and tags, round trips
     uint32_t* acc = XS.acc + (size_t)c * nt;
