@@ -16,6 +16,7 @@ struct tamc_pt::FastState {
   tamc::PtJob job{};
   tamc::DBuf<uint32_t> W;
   tamc::DBuf<double> Ec, Er;
+  tamc::DBuf<char> book;  // the block that betas, tags, acc, rtrips and dhist view
   tamc::DBuf<uint8_t> tags;
   tamc::DBuf<uint32_t> acc, rtrips, dhist;
   tamc::DBuf<float> betas;
@@ -44,6 +45,7 @@ struct tamc_pt::FastState {
 };
 
 bool tamc_pt::fast_plain() const { return fast && fast->plain; }
+bool tamc_pt::fast_deferred() const { return fast && fast->init_pending; }
 
 namespace tamc {
 
@@ -191,25 +193,29 @@ static void fill_job(tamc_pt* pt, uint64_t seed, tamc_pt::FastState* F) {
   F->W.alloc((size_t)j.n * j.nw);
   F->Ec.alloc((size_t)j.C * j.ntp);
   F->Er.alloc((size_t)j.C * j.ntp);
-  F->tags.alloc((size_t)j.C * j.nt);
-  F->acc.alloc((size_t)j.C * j.nt);
-  F->rtrips.alloc(j.C);
-  F->dhist.alloc((size_t)j.C * j.nt * 2);
-  F->betas.alloc(j.ntp);
   F->d_job.alloc(1);
   F->ctr.alloc(1);
-  std::vector<float> b(j.ntp, 0.0f);
-  std::copy(c.betas.begin(), c.betas.end(), b.begin());
-  TAMC_CUDA(tamc::copy_async(F->betas.p, b.data(), j.ntp * 4, cudaMemcpyHostToDevice, st));
-  std::vector<uint8_t> tags((size_t)j.C * j.nt, 0);
+  // the ladder and the exchange bookkeeping in one block, set by one copy:
+  // betas padded with beta = 0, round-trip tags (1 at the lowest slot, 2 at
+  // the highest, per chain), zero acceptance counts, round trips and
+  // diffusion histograms
+  const size_t CT = (size_t)j.C * j.nt;
+  auto a16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+  const size_t o_acc = a16((size_t)j.ntp * 4), o_rt = o_acc + a16(CT * 4), o_dh = o_rt + a16((size_t)j.C * 4),
+               o_tags = o_dh + a16(CT * 8), book_bytes = o_tags + a16(CT);
+  std::vector<char> hb(book_bytes, 0);
+  std::copy(c.betas.begin(), c.betas.end(), reinterpret_cast<float*>(hb.data()));
   for (uint32_t ch = 0; ch < j.C; ++ch) {
-    tags[(size_t)ch * j.nt] = 1;
-    tags[(size_t)ch * j.nt + j.nt - 1] = 2;
+    hb[o_tags + (size_t)ch * j.nt] = 1;
+    hb[o_tags + (size_t)ch * j.nt + j.nt - 1] = 2;
   }
-  TAMC_CUDA(tamc::copy_async(F->tags.p, tags.data(), tags.size(), cudaMemcpyHostToDevice, st));
-  F->acc.zero(st);
-  F->rtrips.zero(st);
-  F->dhist.zero(st);
+  F->book.alloc(book_bytes);
+  TAMC_CUDA(tamc::copy_async(F->book.p, hb.data(), book_bytes, cudaMemcpyHostToDevice, st));
+  F->betas.view(F->book.p, j.ntp);
+  F->acc.view(F->book.p + o_acc, CT);
+  F->rtrips.view(F->book.p + o_rt, j.C);
+  F->dhist.view(F->book.p + o_dh, CT * 2);
+  F->tags.view(F->book.p + o_tags, CT);
   j.betas = F->betas.p;
   j.W = F->W.p;
   j.Ec = F->Ec.p;

@@ -54,15 +54,15 @@ void PtOutputs::init(const PtCfg& c, uint32_t n_, uint32_t nchi_, cudaStream_t s
   samp.alloc((size_t)c.Z * c.S * c.C * ((n + 7) / 8));
   const uint32_t tracked = c.num_sweeps > c.meas_init ? c.num_sweeps - c.meas_init : 0;
   cap = std::max(1u, std::min(tracked, 1024u));
-  gs_count.alloc(1);
-  gs_have.alloc(1);
-  gs_min.alloc(1);
+  // count, have and running minimum start at zero: one block, one memset
+  gs_cells.alloc(16);
+  gs_count.view(gs_cells.p, 1);
+  gs_have.view(gs_cells.p + 4, 1);
+  gs_min.view(gs_cells.p + 8, 1);
+  gs_cells.zero(st);
   gs_steps.alloc(cap);
   gs_E.alloc(cap);
   gs_words.alloc((size_t)cap * ((n + 63) / 64));
-  gs_count.zero(st);
-  gs_have.zero(st);
-  gs_min.zero(st);
 }
 
 MeasOut PtOutputs::meas(const PtCfg& c) const {
@@ -275,7 +275,10 @@ int tamc_gpu_pt_create(tamc_inst* inst, const tamc_pt_params* p, uint64_t seed, 
     pt->out.init(pt->cfg, inst->n, inst->nchi, pt->g->stream);
     if (mode == TAMC_MODE_REF) ref_create(pt, xo_seed_from_u64(seed));
     else fast_pt_create(pt, seed);
-    TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
+    // a batch run has launched nothing yet (its copies read pageable host
+    // memory, which cudaMemcpyAsync stages before returning): no wait; the
+    // batch's first chunk launch reports any error
+    if (!pt->fast_deferred()) TAMC_CUDA(cudaStreamSynchronize(pt->g->stream));
   } catch (...) {
     if (pt->fast) fast_pt_destroy(pt);
     delete pt;

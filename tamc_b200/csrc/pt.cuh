@@ -9,21 +9,31 @@
 namespace tamc {
 
 template <class T>
-struct DBuf {  // owning device buffer
+struct DBuf {  // owning device buffer, or a view into another buffer's block
   T* p = nullptr;
   size_t n = 0;
+  bool own = true;
   DBuf() = default;
   explicit DBuf(size_t count) { alloc(count); }
-  void alloc(size_t count) {
-    if (p) dev_free(p, std::max<size_t>(n, 1) * sizeof(T));
+  void release() {
+    if (p && own) dev_free(p, std::max<size_t>(n, 1) * sizeof(T));
     p = nullptr;
+  }
+  void alloc(size_t count) {
+    release();
+    own = true;
     n = count;
     p = static_cast<T*>(dev_alloc(std::max<size_t>(count, 1) * sizeof(T)));
   }
-  void zero(cudaStream_t st) { TAMC_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), st)); }
-  ~DBuf() {
-    if (p) dev_free(p, std::max<size_t>(n, 1) * sizeof(T));
+  // `count` elements at `q`, inside a block that another DBuf owns and frees
+  void view(void* q, size_t count) {
+    release();
+    own = false;
+    n = count;
+    p = static_cast<T*>(q);
   }
+  void zero(cudaStream_t st) { TAMC_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), st)); }
+  ~DBuf() { release(); }
   DBuf(const DBuf&) = delete;
   DBuf& operator=(const DBuf&) = delete;
 };
@@ -57,6 +67,7 @@ struct PtOutputs {
   DBuf<int32_t> q;
   DBuf<float> sus;
   DBuf<uint8_t> samp;
+  DBuf<char> gs_cells;  // one block holding the three cells below
   DBuf<uint32_t> gs_count;
   DBuf<int> gs_have;
   DBuf<float> gs_min;
@@ -115,4 +126,5 @@ struct tamc_pt {
   struct FastState;
   FastState* fast = nullptr;
   bool fast_plain() const;  // the run uses the all-SM plain form
+  bool fast_deferred() const;  // a batch run whose initial replicas wait for the batch's first chunk
 };
