@@ -1501,22 +1501,27 @@ __device__ __forceinline__ void load_job(PtJob& dst, const PtJob* src) {
 
 // The fused job's bookkeeping into shared memory (start of a range of rounds)
 // and back (its end); the end also reports the log count.
-__device__ __noinline__ void xchg_load(const PtJob& J, char* xb, bool gs = true) {
+// Threads from t0 on copy (the ones below t0 may be loading something else
+// meanwhile); every thread meets the closing barrier.
+__device__ __noinline__ void xchg_load(const PtJob& J, char* xb, bool gs = true, uint32_t t0 = 0) {
   XchgSm X;
   xchg_layout(&X, xb, J.C, J.ntp);
   const uint32_t CT = J.C * J.nt;
-  for (uint32_t x = threadIdx.x; x < CT; x += blockDim.x) {
-    X.tags[x] = J.tags[x];
-    X.acc[x] = J.acc[x];
-    X.dhist[2 * x] = J.dhist[2 * x];
-    X.dhist[2 * x + 1] = J.dhist[2 * x + 1];
-  }
-  for (uint32_t c = threadIdx.x; c < J.C; c += blockDim.x) X.rtrips[c] = J.rtrips[c];
-  for (uint32_t j = threadIdx.x; j + 1 < J.nt; j += blockDim.x) X.dbeta[j] = J.betas[j + 1] - J.betas[j];
-  if (gs && threadIdx.x == 0) {
-    X.gs->have = *J.log.have;
-    X.gs->minE = *J.log.minE;
-    X.gs->count = *J.log.count;
+  if (threadIdx.x >= t0) {
+    const uint32_t tid = threadIdx.x - t0, T = blockDim.x - t0;
+    for (uint32_t x = tid; x < CT; x += T) {
+      X.tags[x] = J.tags[x];
+      X.acc[x] = J.acc[x];
+      X.dhist[2 * x] = J.dhist[2 * x];
+      X.dhist[2 * x + 1] = J.dhist[2 * x + 1];
+    }
+    for (uint32_t c = tid; c < J.C; c += T) X.rtrips[c] = J.rtrips[c];
+    for (uint32_t j = tid; j + 1 < J.nt; j += T) X.dbeta[j] = J.betas[j + 1] - J.betas[j];
+    if (gs && tid == 0) {
+      X.gs->have = *J.log.have;
+      X.gs->minE = *J.log.minE;
+      X.gs->count = *J.log.count;
+    }
   }
   __syncthreads();
 }
@@ -1749,7 +1754,7 @@ __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict_
 }
 
 __device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long long* icm_dE, uint32_t* icm_valid,
-                                    char* base, unsigned long long* dm);
+                                    char* base, unsigned long long* dm, bool staged = false);
 
 // Houdayer moves of round ctl->i: one CTA per (chain pair, slot >= lo).
 __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__ jp, PlainCtl* ctl, long long* icm_dE,
@@ -1924,10 +1929,34 @@ __device__ __forceinline__ int bar1_or(int pred, uint32_t count) {
   return r;
 }
 
+// Stages the exchange's inputs into `base` in plain_exchange_body's layout:
+// the energies as the round started (the Houdayer changes are added at the
+// exchange) and the bookkeeping that xchg_load copies, by the threads tid of
+// T (part of the CTA; no barrier).
+__device__ void plain_exch_stage(const PtJob& J, char* base, uint32_t tid, uint32_t T) {
+  const uint32_t CN = J.C * J.ntp, CT = J.C * J.nt;
+  double* Ec = (double*)base;
+  double* Er = (double*)(base + al16((size_t)CN * 8));
+  for (uint32_t x = tid; x < CN; x += T) {
+    Ec[x] = J.Ec[x];
+    Er[x] = J.Er[x];
+  }
+  XchgSm X;
+  xchg_layout(&X, base + plain_head_smem(J.n, J.C, J.ntp), J.C, J.ntp);
+  for (uint32_t x = tid; x < CT; x += T) {
+    X.tags[x] = J.tags[x];
+    X.acc[x] = J.acc[x];
+    X.dhist[2 * x] = J.dhist[2 * x];
+    X.dhist[2 * x + 1] = J.dhist[2 * x + 1];
+  }
+  for (uint32_t c = tid; c < J.C; c += T) X.rtrips[c] = J.rtrips[c];
+  for (uint32_t j = tid; j + 1 < J.nt; j += T) X.dbeta[j] = J.betas[j + 1] - J.betas[j];
+}
+
 template <uint32_t L, uint32_t DIM>
 __global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restrict__ jp, PlainCtl* ctl,
                                                            long long* icm_dE, uint32_t* icm_valid,
-                                                           unsigned long long* dm) {
+                                                           unsigned long long* dm, int stage_exch) {
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -1947,7 +1976,7 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restri
   const uint32_t nnz = J.F.nnz;
   char* base = reinterpret_cast<char*>(smem_u4);
   LatScratch X;
-  carve_lat(&X, base, n, nnz);
+  char* const xbase = base + carve_lat(&X, base, n, nnz);  // the exchange's staged inputs (stage_exch)
   uint32_t* const Wg = J.W;
   PhaseClock pc;  // with profiling on, cycles are summed over the CTAs
   pc.start(J.prof);
@@ -2085,6 +2114,9 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restri
     copy16(X.cols, J.F.fcolt, nnz / 8);
     copy16(X.bias, J.F.bias, n / 4);
     copy16(X.perm, J.F.perm, n / 4);
+    // every CTA stages the exchange's inputs (only the last one uses them), so
+    // that the exchange reads just the Houdayer changes from L2
+    if (stage_exch) plain_exch_stage(J, xbase, st, ns);
     asm volatile("cp.async.wait_all;\n" ::: "memory");
   }
   __syncthreads();
@@ -2104,13 +2136,25 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restri
     auto bit = [](const uint32_t* m, uint32_t s) { return (m[s >> 5] >> (s & 31u)) & 1u; };
     for (uint32_t s = tid; s < n; s += T) {
       if (!bit(X.Ccol, s)) continue;
+      // every neighbour's column, coupling and bits loaded before the sum
+      uint32_t jj[DEG], cw[DEG], rw[DEG];
+      float Jv[DEG];
+#pragma unroll
+      for (uint32_t m = 0; m < DEG; ++m) {
+        jj[m] = X.cols[m * n + s];
+        Jv[m] = X.Jf[m * n + s];
+      }
+#pragma unroll
+      for (uint32_t m = 0; m < DEG; ++m) {
+        cw[m] = X.Ccol[jj[m] >> 5];
+        rw[m] = X.R0col[jj[m] >> 5];
+      }
       float f0 = X.bias[s];
 #pragma unroll
       for (uint32_t m = 0; m < DEG; ++m) {
-        const uint32_t jj = X.cols[m * n + s];
-        if (jj == s || bit(X.Ccol, jj)) continue;
-        const float Jv = X.Jf[m * n + s];
-        f0 += bit(X.R0col, jj) ? -Jv : Jv;
+        const uint32_t sh = jj[m] & 31u;
+        if (jj[m] == s || ((cw[m] >> sh) & 1u)) continue;
+        f0 += ((rw[m] >> sh) & 1u) ? -Jv[m] : Jv[m];
       }
       const float s0 = bit(X.R0col, s) ? -1.0f : 1.0f;
       a0 += to_fx(-2.0f * s0 * f0);
@@ -2119,8 +2163,12 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restri
     for (int off = 16; off > 0; off >>= 1) a0 += __shfl_xor_sync(0xffffffffu, a0, off);
     if (lane == 0) X.part[warp] = a0;
     __syncthreads();
-    a0 = 0;
-    for (uint32_t k = 0; k < nwarp; ++k) a0 += X.part[k];
+    if (warp == 0) {  // only thread 0 uses the total (integers: any order)
+      a0 = 0;
+      for (uint32_t k = lane; k < nwarp; k += 32) a0 += X.part[k];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+    }
     pc.lap(PHASE_ICM_MARK);
     // flip the cluster in both replicas
     for (uint32_t s = tid; s < n; s += T)
@@ -2149,7 +2197,7 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restri
   if (!s_last) return;
   __threadfence();
   if (tid == 0) ctl->icm_done = 0;
-  plain_exchange_body(J, ctl, icm_dE, icm_valid, base, dm);
+  plain_exchange_body(J, ctl, icm_dE, icm_valid, stage_exch ? xbase : base, dm, stage_exch != 0);
 }
 
 // Houdayer moves of round ctl->i on thread-block clusters: one cluster of CL
@@ -2419,17 +2467,21 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm_cl(const PtJob* __restric
 // Energies after the Houdayer moves and the exchange decisions of round
 // ctl->i (the spin permutation follows in k_plain_perm); advances ctl->i.
 // `base` is shared memory for Ec, Er and Dm; dm receives Dm for k_plain_perm.
+// With `staged`, the energies (without this round's Houdayer changes) and the
+// exchange bookkeeping are already in `base`'s layout (plain_exch_stage): only
+// the Houdayer changes are read from global memory.
 __device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long long* icm_dE, uint32_t* icm_valid,
-                                    char* base, unsigned long long* dm) {
+                                    char* base, unsigned long long* dm, bool staged) {
   const uint32_t tid = threadIdx.x;
   Smem S{};
   S.Ec = (double*)base;
   S.Er = (double*)(base + al16((size_t)J.C * J.ntp * 8));
   S.Dm = (unsigned long long*)(base + 2 * al16((size_t)J.C * J.ntp * 8));
   S.W = J.W;
+  S.xb = base + plain_head_smem(J.n, J.C, J.ntp);
   const uint32_t CN = J.C * J.ntp;
   for (uint32_t x = tid; x < CN; x += blockDim.x) {
-    double ec = J.Ec[x], er = J.Er[x];
+    double ec = staged ? S.Ec[x] : J.Ec[x], er = staged ? S.Er[x] : J.Er[x];
     // written by other CTAs of the Houdayer kernel: read through L2
     if (J.icm && __ldcg(icm_valid + x)) {  // invalidated caches are recomputed as energy_ref
       er += (double)__ldcg(icm_dE + x) * TAMC_FX_INV;
@@ -2439,11 +2491,16 @@ __device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long lo
     S.Ec[x] = ec;
     S.Er[x] = er;
   }
-  __syncthreads();
-  // the exchange bookkeeping in shared memory: one round of parallel global
-  // loads and stores instead of dependent global round trips in the decisions
-  S.xb = base + plain_head_smem(J.n, J.C, J.ntp);
-  xchg_load(J, S.xb, false);
+  if (staged) {
+    __syncthreads();
+  } else {
+    // the exchange bookkeeping in shared memory: one round of parallel global
+    // loads and stores instead of dependent global round trips in the decisions;
+    // staged by the threads above the energies' so that both sets of loads are
+    // in flight together (its closing barrier covers the energies too)
+    const uint32_t t0 = (CN + 31) / 32 * 32;
+    xchg_load(J, S.xb, false, t0 + 32 <= blockDim.x ? t0 : 0);
+  }
   PhaseClock pc;
   pc.start(J.prof);
   const uint32_t i = ctl->i;
@@ -2864,12 +2921,18 @@ static bool plain_launch_icm_lattice(cudaStream_t st, const PtJob& j, const PtJo
     if (e[0] == '0') return false;
   const uint32_t L = j.F.lat_L, dim = j.F.udeg / 2;
   if (!L || j.icm_uf || !j.F.fJt || !j.F.fcolt || (dim != 2 && dim != 3)) return false;
-  const size_t smem = std::max(carve_lat(nullptr, nullptr, j.n, j.F.nnz), plain_exch_smem(j.n, j.C, j.ntp));
-  if (smem > smem_limit || j.n / 32 >= 1024) return false;
+  const size_t lat = carve_lat(nullptr, nullptr, j.n, j.F.nnz), exch = plain_exch_smem(j.n, j.C, j.ntp);
+  if (std::max(lat, exch) > smem_limit || j.n / 32 >= 1024) return false;
+  // the exchange's inputs staged beside the search scratch when both fit
+  // (TAMC_PLAIN_XSTAGE=0: the exchange loads them itself)
+  int stage_exch = lat + exch <= smem_limit;
+  if (const char* e = getenv("TAMC_PLAIN_XSTAGE"))
+    if (e[0] == '0') stage_exch = 0;
+  const size_t smem = stage_exch ? lat + exch : std::max(lat, exch);
   const uint32_t grid = (j.C / 2) * (j.nt - j.lo);
   auto go = [&](auto k) {
     TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, dm);
+    k<<<grid, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, dm, stage_exch);
     TAMC_CUDA(cudaGetLastError());
   };
   if (L == 16 && dim == 2) go(k_plain_icm_lat<16, 2>);

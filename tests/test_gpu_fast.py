@@ -536,8 +536,10 @@ def test_plain_lattice_bitmap_houdayer_identical_to_site_words(tb, po, gpu, monk
     Houdayer move runs on site bitmaps in file order (word-parallel growth,
     couplings staged in shared memory); the chain is the one of the site-word
     kernel (TAMC_PLAIN_LATTICE=0): states, energies, ground-state log, samples,
-    acceptance and round trips bit for bit.  L = 12 is not a lattice of that
-    kind and takes the site-word kernel either way."""
+    acceptance and round trips bit for bit, with the exchange's inputs staged
+    in the Houdayer CTAs' shared memory or loaded by the exchange itself
+    (TAMC_PLAIN_XSTAGE=0).  L = 12 is not a lattice of that kind and takes the
+    site-word kernel either way."""
     if kind == "2d_L16_pm_C1":
         text, nt, C, sweeps = gi.lattice(16, 2, "pm", 0), 32, 2, 60
     elif kind == "2d_L32_gauss":
@@ -551,14 +553,16 @@ def test_plain_lattice_bitmap_houdayer_identical_to_site_words(tb, po, gpu, monk
     d = gpu.upload(tb.HostInstance.parse(text))
     monkeypatch.setenv("TAMC_PT_FORM", "plain")
     out = []
-    for lat in ("1", "0"):
+    for lat, xs in (("1", "1"), ("1", "0"), ("0", "1")):
         monkeypatch.setenv("TAMC_PLAIN_LATTICE", lat)
+        monkeypatch.setenv("TAMC_PLAIN_XSTAGE", xs)
         r = tb.PtRun(d, p, 91).run().sync()
         ts = r.samples()
         out.append([*r.state(), *r.gs(), np.array(ts.e), np.array(ts.q), np.array(ts.samples), r.acceptance(),
                     *r.round_trips()])
-    for a, c in zip(out[0], out[1]):
-        assert np.array_equal(a, c)
+    for o in out[1:]:
+        for a, c in zip(out[0], o):
+            assert np.array_equal(a, c)
     assert out[0][3].size > 0 and np.any(out[0][-3] > 0)  # a ground-state log and accepted exchanges
 
 
