@@ -2083,10 +2083,9 @@ __global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restri
         int g = 0;
         if (own && d != c) {
           const uint32_t c_in = c;
-          c = lat_close<L>(c, d);  // closure inside the word
           uint32_t nb = L == 16 ? (X.Co[wym] >> 16) | (X.Co[wyp] << 16) : X.Co[wym] | X.Co[wyp];
           if (DIM == 3) nb |= X.Co[wxm] | X.Co[wxp];
-          c |= d & nb;
+          c = lat_close<L>(c | (d & nb), d);  // the neighbours' bits, then the closure inside the word
           if (c != c_in) {
             X.Co[wi] = c;
             g = 1;
