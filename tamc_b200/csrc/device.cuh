@@ -49,6 +49,19 @@ void dev_free(void* p, size_t bytes);
 // Returns the cached blocks of `device` to the driver.
 void dev_cache_release(int device);
 
+// Programmatic dependent launch: a kernel launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization may be scheduled while
+// the kernel before it in the stream still runs.  It calls this first, on
+// every path: wait until that kernel has completed and its writes are
+// visible, then let the next kernel of the stream be scheduled.  A kernel so
+// launched therefore completes only after its predecessor did, and the
+// launch latency of each kernel overlaps the one before it.  Launched without
+// the attribute, both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // ------------------------------------------------------------ RNG ----
 // Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): ten rounds of the
 // multiply-hi/lo Feistel round with multipliers 0xD2511F53 / 0xCD9E8D57 and

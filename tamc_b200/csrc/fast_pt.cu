@@ -1665,6 +1665,7 @@ __host__ __device__ inline size_t plain_exch_smem(uint32_t n, uint32_t C, uint32
 // (mode 2) set the initial energies from the energy kernel's sums.
 __global__ void __launch_bounds__(1024, 1) k_plain_head(const PtJob* __restrict__ jp, PlainCtl* ctl,
                                                        long long* acc, int mode, int stage) {
+  pdl_enter();
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -1759,6 +1760,7 @@ __device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long lo
 // Houdayer moves of round ctl->i: one CTA per (chain pair, slot >= lo).
 __global__ void __launch_bounds__(1024, 1) k_plain_icm(const PtJob* __restrict__ jp, PlainCtl* ctl, long long* icm_dE,
                                                        uint32_t* icm_valid, int stage, unsigned long long* dm) {
+  pdl_enter();
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -1957,6 +1959,7 @@ template <uint32_t L, uint32_t DIM>
 __global__ void __launch_bounds__(1024, 1) k_plain_icm_lat(const PtJob* __restrict__ jp, PlainCtl* ctl,
                                                            long long* icm_dE, uint32_t* icm_valid,
                                                            unsigned long long* dm, int stage_exch) {
+  pdl_enter();
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -2264,6 +2267,7 @@ template <uint32_t CL, uint32_t DEG, uint32_t PS>
 __global__ void __launch_bounds__(1024, 1) k_plain_icm_cl(const PtJob* __restrict__ jp, PlainCtl* ctl,
                                                           long long* icm_dE, uint32_t* icm_valid,
                                                           unsigned long long* dm) {
+  pdl_enter();
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -2522,6 +2526,7 @@ __device__ void plain_exchange_body(const PtJob& J, PlainCtl* ctl, const long lo
 __global__ void __launch_bounds__(1024, 1) k_plain_exch(const PtJob* __restrict__ jp, PlainCtl* ctl,
                                                        const long long* icm_dE, uint32_t* icm_valid,
                                                        unsigned long long* dm) {
+  pdl_enter();
   extern __shared__ uint4 smem_u4[];
   __shared__ PtJob s_J;
   load_job(s_J, jp);
@@ -2530,6 +2535,7 @@ __global__ void __launch_bounds__(1024, 1) k_plain_exch(const PtJob* __restrict_
 
 // Spin permutation of the exchange: one thread per (site, chain) word pair.
 __global__ void __launch_bounds__(256) k_plain_perm(const PtJob* __restrict__ jp, const unsigned long long* dm) {
+  pdl_enter();
   const PtJob& J = *jp;
   const uint32_t C = J.C, wpc = J.wpc, nw = J.nw;
   uint32_t* const W = J.W;
@@ -2597,6 +2603,7 @@ __device__ void plain_close_round(const PtJob& J, PlainCtl* ctl, long long* acc,
 template <bool SELF, uint32_t DEG, bool CLOSE>
 __global__ void __launch_bounds__(256, 3) k_plain_sweep(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
                                                      long long* acc) {
+  pdl_enter();
   extern __shared__ uint4 smem_u4[];
   const PtJob& J = *jp;
   Fx4* red = reinterpret_cast<Fx4*>(smem_u4);                 // [blockDim.x]
@@ -2697,6 +2704,7 @@ __global__ void __launch_bounds__(256, 3) k_plain_sweep(const PtJob* __restrict_
 template <uint32_t DEG, bool CLOSE>
 __global__ void __launch_bounds__(256, 3) k_plain_sweep_msc(const PtJob* __restrict__ jp, PlainCtl* ctl, uint32_t color,
                                                          long long* acc) {
+  pdl_enter();
   extern __shared__ uint4 smem_u4[];
   const PtJob& J = *jp;
   const uint32_t nw = J.nw;
@@ -2828,11 +2836,39 @@ size_t plain_head_bytes(const PtJob& j, bool stage) {
   return b;
 }
 
+// Launches of the plain form's rounds: each kernel may be scheduled while the
+// one before it in the stream still runs (programmatic dependent launch; the
+// kernels begin with pdl_enter).  TAMC_PDL=0 launches them in plain stream
+// order.  Both give the same results: pdl_enter orders every kernel after its
+// predecessor.
+static bool pdl_on() {
+  static const bool on = [] {
+    const char* e = getenv("TAMC_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+static void plain_launch(void (*k)(KArgs...), uint32_t grid, uint32_t block, size_t smem, cudaStream_t st,
+                         Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_on() ? 1 : 0;
+  TAMC_CUDA(cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...));
+}
+
 void plain_launch_head(cudaStream_t st, const PtJob* d_job, PlainCtl* ctl, long long* acc, int mode, size_t smem,
                        int stage) {
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_head, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_plain_head<<<1, 1024, smem, st>>>(d_job, ctl, acc, mode, stage);
-  TAMC_CUDA(cudaGetLastError());
+  plain_launch(k_plain_head, 1, 1024, smem, st, d_job, ctl, acc, mode, stage);
 }
 
 // Shared memory of the plain Houdayer kernel with the given staging (bit 0:
@@ -2859,13 +2895,15 @@ static void launch_icm_cl(cudaStream_t st, uint32_t nclusters, size_t smem, cons
   cfg.blockDim = dim3(1024);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = CL;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = pdl_on() ? 2 : 1;
   TAMC_CUDA(cudaLaunchKernelEx(&cfg, k, d_job, ctl, icm_dE, icm_valid, dm));
 }
 
@@ -2931,8 +2969,7 @@ static bool plain_launch_icm_lattice(cudaStream_t st, const PtJob& j, const PtJo
   const uint32_t grid = (j.C / 2) * (j.nt - j.lo);
   auto go = [&](auto k) {
     TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, dm, stage_exch);
-    TAMC_CUDA(cudaGetLastError());
+    plain_launch(k, grid, 1024, smem, st, d_job, ctl, icm_dE, icm_valid, dm, stage_exch);
   };
   if (L == 16 && dim == 2) go(k_plain_icm_lat<16, 2>);
   else if (L == 16 && dim == 3) go(k_plain_icm_lat<16, 3>);
@@ -2953,8 +2990,7 @@ bool plain_launch_icm(cudaStream_t st, const PtJob& j, const PtJob* d_job, Plain
   if (plain_icm_smem(j, stage) > smem_limit) stage = 0;
   const size_t smem = plain_icm_smem(j, stage);
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_icm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_plain_icm<<<grid, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, stage, dm);
-  TAMC_CUDA(cudaGetLastError());
+  plain_launch(k_plain_icm, grid, 1024, smem, st, d_job, ctl, icm_dE, icm_valid, stage, dm);
   return true;
 }
 
@@ -2962,16 +2998,14 @@ void plain_launch_exch(cudaStream_t st, const PtJob& j, const PtJob* d_job, Plai
                        uint32_t* icm_valid, unsigned long long* dm) {
   const size_t smem = plain_exch_smem(j.n, j.C, j.ntp);
   TAMC_CUDA(cudaFuncSetAttribute(k_plain_exch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_plain_exch<<<1, 1024, smem, st>>>(d_job, ctl, icm_dE, icm_valid, dm);
-  TAMC_CUDA(cudaGetLastError());
+  plain_launch(k_plain_exch, 1, 1024, smem, st, d_job, ctl, icm_dE, icm_valid, dm);
 }
 
 void plain_launch_perm(cudaStream_t st, const PtJob& j, const PtJob* d_job, const unsigned long long* dm,
                        uint32_t grid_cap) {
   const uint64_t total = (uint64_t)j.n * j.C;
   const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(grid_cap, (total + 255) / 256));
-  k_plain_perm<<<grid, 256, 0, st>>>(d_job, dm);
-  TAMC_CUDA(cudaGetLastError());
+  plain_launch(k_plain_perm, grid, 256, 0, st, d_job, dm);
 }
 
 template <bool CLOSE>
@@ -2979,7 +3013,7 @@ static void plain_launch_sweep_t(cudaStream_t st, const PtJob& j, const PtJob* d
                                  uint32_t color, uint32_t grid, uint32_t T, size_t smem, long long* acc) {
   auto go = [&](auto k) {
     TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, T, smem, st>>>(d_job, ctl, color, acc);
+    plain_launch(k, grid, T, smem, st, d_job, ctl, color, acc);
   };
   const uint32_t deg = j.F.udeg == 4 || j.F.udeg == 6 ? j.F.udeg : 0;
   if (j.self_loops) {
@@ -3006,7 +3040,7 @@ void plain_launch_sweep(cudaStream_t st, const PtJob& j, const PtJob* d_job, Pla
                         (last ? 2 * al16((size_t)j.C * j.ntp * 8) : 0);
     auto go = [&](auto k) {
       TAMC_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k<<<grid, T, smem, st>>>(d_job, ctl, color, acc);
+      plain_launch(k, grid, T, smem, st, d_job, ctl, color, acc);
     };
     if (j.F.udeg == 4) {
       if (last) go(k_plain_sweep_msc<4, true>);
