@@ -566,6 +566,49 @@ def test_plain_lattice_bitmap_houdayer_identical_to_site_words(tb, po, gpu, monk
     assert out[0][3].size > 0 and np.any(out[0][-3] > 0)  # a ground-state log and accepted exchanges
 
 
+@pytest.mark.parametrize("kind", ["3d_L16_gauss_C4", "2d_L12_pm"])
+def test_plain_programmatic_launches_identical_to_stream_order(tb, po, gpu, monkeypatch, kind):
+    """The plain form's round kernels are launched so that each may start
+    while the one before it still runs, and wait inside for its completion;
+    the chain is the one of launches in plain stream order (TAMC_PDL=0):
+    states, energies, ground-state log, samples, acceptance and round trips
+    bit for bit.  The switch is read once per process, so the stream-order
+    run is a child process."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = r'''
+import json, sys
+import numpy as np
+import tamc_b200 as tb
+from tamc_b200 import instances as gi
+kind = sys.argv[1]
+if kind == "3d_L16_gauss_C4":
+    text, nt, sweeps = gi.lattice(16, 3, "gauss", 0), 64, 30
+else:
+    text, nt, sweeps = gi.lattice(12, 2, "pm", 4), 24, 40
+b = tb.geometric_betas(0.2, 5.0, nt)
+lo = int(np.argmax(b >= np.float32(1.0)))
+p = tb.PtParams(sweeps, b, lo, 0.0, True, 2, 8, 5, 7, 0)
+d = tb.Gpu(0).upload(tb.HostInstance.parse(text))
+r = tb.PtRun(d, p, 91).run().sync()
+ts = r.samples()
+out = [*r.state(), *r.gs(), np.array(ts.e), np.array(ts.q), np.array(ts.samples), r.acceptance(), *r.round_trips()]
+print(json.dumps([np.asarray(a).tobytes().hex() for a in out]))
+'''
+    res = []
+    for pdl in ("1", "0"):
+        env = dict(os.environ, TAMC_PT_FORM="plain", TAMC_PDL=pdl)
+        cp = subprocess.run([sys.executable, "-c", script, kind], env=env, capture_output=True, text=True,
+                            timeout=600, cwd=root)
+        assert cp.returncode == 0, cp.stderr[-2000:]
+        res.append(json.loads(cp.stdout.strip().splitlines()[-1]))
+    assert res[0] == res[1]
+    assert len(res[0][3]) > 0  # a ground-state log
+
+
 @pytest.mark.parametrize("kind", ["3d_L8_64", "2d_L32_32", "3d_L16_64_c4"])
 def test_plain_cluster_houdayer_kernel_identical_to_one_cta(tb, po, gpu, monkeypatch, kind):
     """The plain form's Houdayer move on 2- or 4-CTA clusters (sites split over
