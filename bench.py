@@ -394,12 +394,12 @@ def run_c3(args):
         gpu.sync()
         c0 = tb.copy_bytes()
         t0 = time.perf_counter()
-        di = [gpu.upload(h) for h in hosts]
+        di = gpu.upload_many(hosts)
         b = tb.Batch(gpu)
         for j, (d, p) in enumerate(zip(di, params)):
             b.add(d, p, jobs[j][3] + 31 * k)
         b.run()
-        res = [(b.gs(j), b.acceptance(j)) for j in range(len(jobs))]
+        res = list(zip(b.gs_all(), b.acceptance_all()))
         del b, di
         gpu.sync()
         t1 = time.perf_counter()
@@ -437,8 +437,8 @@ def run_c3(args):
                "flips_per_step": flips,
                "e2e": {"value": e2e_value, "unit": "flips/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(d2h),
-                       "path": "tamc_gpu_instance_upload x256, tamc_gpu_batch_create/add/run, "
-                               "tamc_gpu_batch_gs + tamc_gpu_batch_acceptance per job, destroy; wall clock",
+                       "path": "tamc_gpu_instance_upload_many (256 instances), tamc_gpu_batch_create/add/run, "
+                               "tamc_gpu_batch_gs_all + tamc_gpu_batch_acceptance_all, destroy; wall clock",
                        "s_per_step": float(e2e_t.item())},
                "gpu_launches": int(launches),
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

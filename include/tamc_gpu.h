@@ -147,6 +147,16 @@ void tamc_copy_bytes(uint64_t* h2d, uint64_t* d2h);
  * the fast mode and the susceptibility weights.  An instance with no sites is
  * refused with TAMC_E_INVAL. */
 int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* h, tamc_inst** out);
+/* Uploads `count` instances at once, as `count` calls of
+ * tamc_gpu_instance_upload would (outs[k] for his[k]), with the host-side
+ * preparation (colouring, re-layouts) spread over up to 16 threads.  For
+ * callers that upload many instances together, such as the instances of one
+ * batch or GLA's sub-instances, which the reference builds all before it runs
+ * them (src/gla.rs:137-153).  All or nothing: on an error no instance is
+ * returned; a null or empty instance is refused with TAMC_E_INVAL naming its
+ * index. */
+int tamc_gpu_instance_upload_many(tamc_gpu* g, uint32_t count, const tamc_host_instance* const* his,
+                                  tamc_inst** outs);
 int tamc_gpu_instance_destroy(tamc_inst* d);
 
 /* ------------------------------------------------------------------------
@@ -265,6 +275,17 @@ int tamc_gpu_batch_round_trips(tamc_batch* b, uint32_t job, uint8_t* tags, uint3
                                uint32_t* diffusion_hist);
 int tamc_gpu_batch_gs(tamc_batch* b, uint32_t job, uint32_t cap, uint32_t* count, uint32_t* steps,
                       float* energies, uint64_t* states);
+/* Every job's ground-state log in one call: counts[njobs] = entries per job
+ * (always written); with steps/energies/states given, the logs job after job
+ * (entries in job order, each job's states as ceil(n/64) words per entry),
+ * which must fit cap_entries / cap_words.  Same values as tamc_gpu_batch_gs
+ * per job; for callers that read a whole batch (no reference counterpart:
+ * the reference returns each run's PtIcmMinResults, src/pt.rs:97-103,
+ * 397-412). */
+int tamc_gpu_batch_gs_all(tamc_batch* b, uint64_t cap_entries, uint64_t cap_words, uint32_t* counts,
+                          uint32_t* steps, float* energies, uint64_t* states);
+/* Every job's acceptance counts, job after job (nt per job), within cap. */
+int tamc_gpu_batch_acceptance_all(tamc_batch* b, uint64_t cap, uint32_t* counts);
 int tamc_gpu_batch_samples_dims(tamc_batch* b, uint32_t job, uint32_t* M, uint32_t* S, uint32_t* Z,
                                 uint32_t* nchi);
 int tamc_gpu_batch_samples(tamc_batch* b, uint32_t job, float* e, int32_t* q, float* suscept,

@@ -101,7 +101,10 @@ _SIGS = {
     "tamc_gpu_launch_count": (C.c_uint64, [vp]),
     "tamc_copy_bytes": (None, [u64p, u64p]),
     "tamc_gpu_instance_upload": (C.c_int, [vp, vp, C.POINTER(vp)]),
+    "tamc_gpu_instance_upload_many": (C.c_int, [vp, C.c_uint32, C.POINTER(vp), C.POINTER(vp)]),
     "tamc_gpu_instance_destroy": (C.c_int, [vp]),
+    "tamc_gpu_batch_gs_all": (C.c_int, [vp, C.c_uint64, C.c_uint64, u32p, u32p, f32p, u64p]),
+    "tamc_gpu_batch_acceptance_all": (C.c_int, [vp, C.c_uint64, u32p]),
     "tamc_gpu_pt_create": (C.c_int, [vp, C.POINTER(_PtParams), C.c_uint64, C.c_int, C.POINTER(vp)]),
     "tamc_gpu_pt_run": (C.c_int, [vp, C.c_uint32]),
     "tamc_gpu_pt_sync": (C.c_int, [vp]),
@@ -369,6 +372,16 @@ class Gpu:
     def upload(self, inst: HostInstance) -> "DeviceInstance":
         return DeviceInstance(self, inst)
 
+    def upload_many(self, insts) -> list:
+        """Uploads several instances in one call (tamc_gpu_instance_upload_many:
+        host preparation on several threads), as many upload() calls would."""
+        insts = list(insts)
+        k = len(insts)
+        his = (vp * max(k, 1))(*[i.h for i in insts])
+        outs = (vp * max(k, 1))()
+        _check(lib().tamc_gpu_instance_upload_many(self.h, k, his, outs))
+        return [DeviceInstance(self, i, handle=outs[j]) for j, i in enumerate(insts)]
+
     def close(self):
         if getattr(self, "h", None):
             lib().tamc_gpu_close(self.h)
@@ -380,10 +393,13 @@ class Gpu:
 
 
 class DeviceInstance:
-    def __init__(self, gpu: Gpu, inst: HostInstance):
+    def __init__(self, gpu: Gpu, inst: HostInstance, handle=None):
         self.gpu, self.host = gpu, inst
-        self.h = vp()
-        _check(lib().tamc_gpu_instance_upload(gpu.h, inst.h, C.byref(self.h)))
+        if handle is not None:  # uploaded by Gpu.upload_many
+            self.h = vp(handle)
+        else:
+            self.h = vp()
+            _check(lib().tamc_gpu_instance_upload(gpu.h, inst.h, C.byref(self.h)))
         self.n = inst.n
 
     def __del__(self):
@@ -587,6 +603,38 @@ class Batch:
         a = np.zeros(len(p.betas), np.uint32)
         _check(lib().tamc_gpu_batch_acceptance(self.h, job, _p(a, u32p)))
         return a
+
+    def gs_all(self) -> list:
+        """gs() of every job, read in two calls (tamc_gpu_batch_gs_all)."""
+        nj = len(self.jobs)
+        cnt = np.zeros(max(nj, 1), np.uint32)
+        _check(lib().tamc_gpu_batch_gs_all(self.h, 0, 0, _p(cnt, u32p), None, None, None))
+        wpj = np.array([(d.n + 63) // 64 for d, _ in self.jobs], np.uint64)
+        cnt = cnt[:nj].astype(np.uint64)
+        ne, nwd = int(cnt.sum()), int((cnt * wpj).sum())
+        steps = np.zeros(max(ne, 1), np.uint32)
+        en = np.zeros(max(ne, 1), np.float32)
+        st = np.zeros(max(nwd, 1), np.uint64)
+        _check(lib().tamc_gpu_batch_gs_all(self.h, ne, nwd, _p(np.zeros(max(nj, 1), np.uint32), u32p),
+                                           _p(steps, u32p), _p(en, f32p), _p(st, u64p)))
+        out, eo, wo = [], 0, 0
+        for j in range(nj):
+            c, w = int(cnt[j]), int(wpj[j])
+            out.append((steps[eo:eo + c], en[eo:eo + c], st[wo:wo + c * w].reshape(c, w)))
+            eo += c
+            wo += c * w
+        return out
+
+    def acceptance_all(self) -> list:
+        """acceptance() of every job in one call (tamc_gpu_batch_acceptance_all)."""
+        nts = [len(p.betas) for _, p in self.jobs]
+        a = np.zeros(max(sum(nts), 1), np.uint32)
+        _check(lib().tamc_gpu_batch_acceptance_all(self.h, sum(nts), _p(a, u32p)))
+        out, o = [], 0
+        for nt in nts:
+            out.append(a[o:o + nt])
+            o += nt
+        return out
 
     def set_state(self, job: int, spins) -> None:
         a = np.ascontiguousarray(spins, np.int8)

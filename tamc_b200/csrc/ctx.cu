@@ -3,6 +3,9 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
 
 #include "device.cuh"
 
@@ -78,6 +81,10 @@ struct UploadPack {
     bytes = host.size();
     arena = dev_alloc(bytes);
     TAMC_CUDA(copy_sync(arena, host.data(), bytes, cudaMemcpyHostToDevice));
+    bind(arena);
+  }
+  // the arrays' device addresses inside `arena`
+  void bind(void* arena) {
     for (auto& s : slots) *s.first = static_cast<char*>(arena) + s.second;
   }
 };
@@ -226,6 +233,8 @@ void tamc_gpu_release(tamc_gpu* g) {
   runner_pool_release(g);
   cudaFree(g->d_exp);
   cudaStreamDestroy(g->stream);
+  if (g->up_stream) cudaStreamDestroy(g->up_stream);
+  if (g->up_pin) cudaFreeHost(g->up_pin);
   dev_cache_release(g->device);
   delete g;
 }
@@ -238,6 +247,110 @@ void tamc_inst_release(tamc_inst* d) {
   d->sa_scratch.release();
   delete d;
   tamc_gpu_release(g);
+}
+
+// Host side of an upload: every array of the instance (reference order, ICM
+// graph, colour order, lattice layouts) into `pack`, and the host fields of
+// `d`.  Touches no device state, so uploads of several instances prepare in
+// parallel.
+static void inst_prepare(tamc_inst* d, const HostInstance& h, UploadPack& pack) {
+  d->host = h;
+  d->n = h.n;
+  d->nnz = h.col.size();
+  d->offset = h.offset;
+  d->nchi = (uint32_t)h.suscept.size();
+  d->self_loops = h.has_self_loops();
+  for (uint32_t i = 0; i < h.n; ++i) d->max_deg = std::max(d->max_deg, h.row_ptr[i + 1] - h.row_ptr[i]);
+  pack.add(&d->d_rp, h.row_ptr.data(), h.row_ptr.size());
+  pack.add(&d->d_col, h.col.data(), h.col.size());
+  pack.add(&d->d_J, h.J.data(), h.J.size());
+  pack.add(&d->d_bias, h.bias.data(), h.bias.size());
+  // ICM graph: off-diagonal entries over the petgraph node range
+  d->g_nodes = h.graph_nodes();
+  std::vector<uint32_t> grp(d->g_nodes + 1, 0), gcol;
+  for (uint32_t i = 0; i < d->g_nodes; ++i) {
+    for (uint32_t e = h.row_ptr[i]; e < h.row_ptr[i + 1]; ++e)
+      if (h.col[e] != i) gcol.push_back(h.col[e]);
+    grp[i + 1] = (uint32_t)gcol.size();
+  }
+  pack.add(&d->d_grp, grp.data(), grp.size());
+  pack.add(&d->d_gcol, gcol.data(), gcol.size());
+  std::vector<double> sus((size_t)d->nchi * h.n);
+  for (uint32_t k = 0; k < d->nchi; ++k) std::copy(h.suscept[k].begin(), h.suscept[k].end(), sus.begin() + (size_t)k * h.n);
+  pack.add(&d->d_sus, sus.data(), sus.size());
+  // colour order
+  std::vector<uint32_t> color;
+  h.coloring(d->ncolors, color);
+  if (h.n == 0) d->ncolors = 0;
+  d->color_off.assign(d->ncolors + 1, 0);
+  for (uint32_t i = 0; i < h.n; ++i) d->color_off[color[i] + 1]++;
+  for (uint32_t c = 0; c < d->ncolors; ++c) d->color_off[c + 1] += d->color_off[c];
+  std::vector<uint32_t> fill(d->color_off.begin(), d->color_off.end() - (d->ncolors ? 1 : 0));
+  d->h_perm.assign(h.n, 0);
+  std::vector<uint32_t> iperm(h.n);
+  for (uint32_t i = 0; i < h.n; ++i) {
+    const uint32_t s = fill[color[i]]++;
+    d->h_perm[s] = i;
+    iperm[i] = s;
+  }
+  std::vector<uint32_t> frp(h.n + 1, 0);
+  std::vector<uint2> fent;
+  fent.reserve(h.col.size());
+  std::vector<float> fbias(h.n), fkd(h.n, 0.0f);
+  std::vector<double> fsus((size_t)d->nchi * h.n);
+  for (uint32_t s = 0; s < h.n; ++s) {
+    const uint32_t i = d->h_perm[s];
+    fbias[s] = h.bias[i];
+    for (uint32_t e = h.row_ptr[i]; e < h.row_ptr[i + 1]; ++e) {
+      uint32_t jb;
+      memcpy(&jb, &h.J[e], 4);
+      fent.push_back(make_uint2(iperm[h.col[e]], jb));
+      if (h.col[e] == i) fkd[s] += h.J[e];
+    }
+    frp[s + 1] = (uint32_t)fent.size();
+    for (uint32_t k = 0; k < d->nchi; ++k) fsus[(size_t)k * h.n + s] = h.suscept[k][i];
+  }
+  pack.add(&d->d_color_off, d->color_off.data(), d->color_off.size());
+  pack.add(&d->d_perm, d->h_perm.data(), d->h_perm.size());
+  pack.add(&d->d_iperm, iperm.data(), iperm.size());
+  pack.add(&d->d_frp, frp.data(), frp.size());
+  d->udeg = h.n ? frp[1] : 0;
+  for (uint32_t s = 0; s < h.n && d->udeg; ++s)
+    if (frp[s + 1] - frp[s] != d->udeg) d->udeg = 0;
+  pack.add(&d->d_fent, fent.data(), fent.size());
+  if (h.n <= 65536) {
+    std::vector<uint16_t> c16((fent.size() + 7) / 8 * 8 + 8, 0);
+    for (size_t e = 0; e < fent.size(); ++e) c16[e] = (uint16_t)fent[e].x;
+    pack.add(&d->d_fcol16, c16.data(), c16.size());
+  }
+  // +-J instances (every coupling +-1, no field, no self-coupling, rows of 4 or
+  // 6 entries) take the multi-spin-coded sweep of the colour-ordered mode
+  d->pmj = (d->udeg == 4 || d->udeg == 6) && !d->self_loops;
+  for (uint32_t s = 0; s < h.n && d->pmj; ++s)
+    if (fbias[s] != 0.0f) d->pmj = 0;
+  for (size_t e = 0; e < fent.size() && d->pmj; ++e)
+    if ((fent[e].y & 0x7fffffffu) != 0x3f800000u) d->pmj = 0;  // |J| == 1.0f
+  d->lat_L = lattice_side(h, d->udeg);
+  std::vector<float> fJt;
+  std::vector<uint16_t> fcolt;
+  if (d->lat_L) {
+    // couplings and columns by (neighbour slot, colour row) for the bitmap
+    // Houdayer kernel: contiguous 16-byte staging, conflict-free reads of
+    // the m-th entries of consecutive rows
+    const uint32_t D = d->udeg;
+    fJt.resize(fent.size());
+    fcolt.resize(fent.size());
+    for (uint32_t s = 0; s < h.n; ++s)
+      for (uint32_t m = 0; m < D; ++m) {
+        memcpy(&fJt[(size_t)m * h.n + s], &fent[(size_t)s * D + m].y, 4);
+        fcolt[(size_t)m * h.n + s] = (uint16_t)fent[(size_t)s * D + m].x;
+      }
+    pack.add(&d->d_fJt, fJt.data(), fJt.size());
+    pack.add(&d->d_fcolt, fcolt.data(), fcolt.size());
+  }
+  pack.add(&d->d_fbias, fbias.data(), fbias.size());
+  pack.add(&d->d_fkd, fkd.data(), fkd.size());
+  pack.add(&d->d_fsus, fsus.data(), fsus.size());
 }
 
 extern "C" {
@@ -316,115 +429,97 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
   // launching empty grids
   if (hi->h.n == 0) fail(TAMC_E_INVAL, "instance has no sites");
   TAMC_CUDA(cudaSetDevice(g->device));
-  const HostInstance& h = hi->h;
   auto* d = new tamc_inst();
   d->g = g;
   tamc_gpu_retain(g);
-  d->host = h;
-  d->n = h.n;
-  d->nnz = h.col.size();
-  d->offset = h.offset;
-  d->nchi = (uint32_t)h.suscept.size();
-  d->self_loops = h.has_self_loops();
-  for (uint32_t i = 0; i < h.n; ++i) d->max_deg = std::max(d->max_deg, h.row_ptr[i + 1] - h.row_ptr[i]);
   try {
     UploadPack pack;
-    pack.add(&d->d_rp, h.row_ptr.data(), h.row_ptr.size());
-    pack.add(&d->d_col, h.col.data(), h.col.size());
-    pack.add(&d->d_J, h.J.data(), h.J.size());
-    pack.add(&d->d_bias, h.bias.data(), h.bias.size());
-    // ICM graph: off-diagonal entries over the petgraph node range
-    d->g_nodes = h.graph_nodes();
-    std::vector<uint32_t> grp(d->g_nodes + 1, 0), gcol;
-    for (uint32_t i = 0; i < d->g_nodes; ++i) {
-      for (uint32_t e = h.row_ptr[i]; e < h.row_ptr[i + 1]; ++e)
-        if (h.col[e] != i) gcol.push_back(h.col[e]);
-      grp[i + 1] = (uint32_t)gcol.size();
-    }
-    pack.add(&d->d_grp, grp.data(), grp.size());
-    pack.add(&d->d_gcol, gcol.data(), gcol.size());
-    std::vector<double> sus((size_t)d->nchi * h.n);
-    for (uint32_t k = 0; k < d->nchi; ++k) std::copy(h.suscept[k].begin(), h.suscept[k].end(), sus.begin() + (size_t)k * h.n);
-    pack.add(&d->d_sus, sus.data(), sus.size());
-    // colour order
-    std::vector<uint32_t> color;
-    h.coloring(d->ncolors, color);
-    if (h.n == 0) d->ncolors = 0;
-    d->color_off.assign(d->ncolors + 1, 0);
-    for (uint32_t i = 0; i < h.n; ++i) d->color_off[color[i] + 1]++;
-    for (uint32_t c = 0; c < d->ncolors; ++c) d->color_off[c + 1] += d->color_off[c];
-    std::vector<uint32_t> fill(d->color_off.begin(), d->color_off.end() - (d->ncolors ? 1 : 0));
-    d->h_perm.assign(h.n, 0);
-    std::vector<uint32_t> iperm(h.n);
-    for (uint32_t i = 0; i < h.n; ++i) {
-      const uint32_t s = fill[color[i]]++;
-      d->h_perm[s] = i;
-      iperm[i] = s;
-    }
-    std::vector<uint32_t> frp(h.n + 1, 0);
-    std::vector<uint2> fent;
-    fent.reserve(h.col.size());
-    std::vector<float> fbias(h.n), fkd(h.n, 0.0f);
-    std::vector<double> fsus((size_t)d->nchi * h.n);
-    for (uint32_t s = 0; s < h.n; ++s) {
-      const uint32_t i = d->h_perm[s];
-      fbias[s] = h.bias[i];
-      for (uint32_t e = h.row_ptr[i]; e < h.row_ptr[i + 1]; ++e) {
-        uint32_t jb;
-        memcpy(&jb, &h.J[e], 4);
-        fent.push_back(make_uint2(iperm[h.col[e]], jb));
-        if (h.col[e] == i) fkd[s] += h.J[e];
-      }
-      frp[s + 1] = (uint32_t)fent.size();
-      for (uint32_t k = 0; k < d->nchi; ++k) fsus[(size_t)k * h.n + s] = h.suscept[k][i];
-    }
-    pack.add(&d->d_color_off, d->color_off.data(), d->color_off.size());
-    pack.add(&d->d_perm, d->h_perm.data(), d->h_perm.size());
-    pack.add(&d->d_iperm, iperm.data(), iperm.size());
-    pack.add(&d->d_frp, frp.data(), frp.size());
-    d->udeg = h.n ? frp[1] : 0;
-    for (uint32_t s = 0; s < h.n && d->udeg; ++s)
-      if (frp[s + 1] - frp[s] != d->udeg) d->udeg = 0;
-    pack.add(&d->d_fent, fent.data(), fent.size());
-    if (h.n <= 65536) {
-      std::vector<uint16_t> c16((fent.size() + 7) / 8 * 8 + 8, 0);
-      for (size_t e = 0; e < fent.size(); ++e) c16[e] = (uint16_t)fent[e].x;
-      pack.add(&d->d_fcol16, c16.data(), c16.size());
-    }
-    // +-J instances (every coupling +-1, no field, no self-coupling, rows of 4 or
-    // 6 entries) take the multi-spin-coded sweep of the colour-ordered mode
-    d->pmj = (d->udeg == 4 || d->udeg == 6) && !d->self_loops;
-    for (uint32_t s = 0; s < h.n && d->pmj; ++s)
-      if (fbias[s] != 0.0f) d->pmj = 0;
-    for (size_t e = 0; e < fent.size() && d->pmj; ++e)
-      if ((fent[e].y & 0x7fffffffu) != 0x3f800000u) d->pmj = 0;  // |J| == 1.0f
-    d->lat_L = lattice_side(h, d->udeg);
-    std::vector<float> fJt;
-    std::vector<uint16_t> fcolt;
-    if (d->lat_L) {
-      // couplings and columns by (neighbour slot, colour row) for the bitmap
-      // Houdayer kernel: contiguous 16-byte staging, conflict-free reads of
-      // the m-th entries of consecutive rows
-      const uint32_t D = d->udeg;
-      fJt.resize(fent.size());
-      fcolt.resize(fent.size());
-      for (uint32_t s = 0; s < h.n; ++s)
-        for (uint32_t m = 0; m < D; ++m) {
-          memcpy(&fJt[(size_t)m * h.n + s], &fent[(size_t)s * D + m].y, 4);
-          fcolt[(size_t)m * h.n + s] = (uint16_t)fent[(size_t)s * D + m].x;
-        }
-      pack.add(&d->d_fJt, fJt.data(), fJt.size());
-      pack.add(&d->d_fcolt, fcolt.data(), fcolt.size());
-    }
-    pack.add(&d->d_fbias, fbias.data(), fbias.size());
-    pack.add(&d->d_fkd, fkd.data(), fkd.size());
-    pack.add(&d->d_fsus, fsus.data(), fsus.size());
+    inst_prepare(d, hi->h, pack);
     pack.commit(d->arena, d->arena_bytes);
   } catch (...) {
     tamc_gpu_instance_destroy(d);
     throw;
   }
   *out = d;
+  TAMC_API_END
+}
+
+int tamc_gpu_instance_upload_many(tamc_gpu* g, uint32_t count, const tamc_host_instance* const* his,
+                                  tamc_inst** outs) {
+  TAMC_API_BEGIN
+  if (!g || (count && (!his || !outs))) fail(TAMC_E_INVAL, "null argument");
+  for (uint32_t k = 0; k < count; ++k) {
+    if (!his[k]) fail(TAMC_E_INVAL, "null instance at index " + std::to_string(k));
+    if (his[k]->h.n == 0) fail(TAMC_E_INVAL, "instance at index " + std::to_string(k) + " has no sites");
+  }
+  if (count == 0) return TAMC_OK;
+  TAMC_CUDA(cudaSetDevice(g->device));
+  std::vector<tamc_inst*> ds(count, nullptr);
+  auto drop_all = [&] {
+    if (g->up_stream) cudaStreamSynchronize(g->up_stream);  // no copy still reads the staging block
+    for (tamc_inst* d : ds)
+      if (d) tamc_gpu_instance_destroy(d);
+  };
+  try {
+    for (uint32_t k = 0; k < count; ++k) {
+      ds[k] = new tamc_inst();
+      ds[k]->g = g;
+      tamc_gpu_retain(g);
+    }
+    // on up to 16 threads: host preparation of every instance, then (after
+    // the staging offsets are known) its copy into the pinned staging block
+    std::vector<UploadPack> packs(count);
+    std::vector<size_t> off(count + 1, 0);
+    std::vector<std::exception_ptr> errs(count);
+    const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint32_t nth = std::min({count, hw, 16u});
+    auto parallel = [&](auto&& f) {
+      std::atomic<uint32_t> next{0};
+      auto work = [&] {
+        for (uint32_t k; (k = next.fetch_add(1)) < count;) {
+          try {
+            f(k);
+          } catch (...) {
+            errs[k] = std::current_exception();
+          }
+        }
+      };
+      std::vector<std::thread> pool;
+      for (uint32_t t = 1; t < nth; ++t) pool.emplace_back(work);
+      work();
+      for (auto& th : pool) th.join();
+      for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
+    };
+    parallel([&](uint32_t k) { inst_prepare(ds[k], his[k]->h, packs[k]); });
+    for (uint32_t k = 0; k < count; ++k) off[k + 1] = off[k] + ((packs[k].host.size() + 255) & ~(size_t)255);
+    std::lock_guard<std::mutex> lk(g->up_mu);
+    if (!g->up_stream) TAMC_CUDA(cudaStreamCreateWithFlags(&g->up_stream, cudaStreamNonBlocking));
+    if (off[count] > g->up_pin_bytes) {
+      if (g->up_pin) TAMC_CUDA(cudaFreeHost(g->up_pin));
+      g->up_pin = nullptr;
+      g->up_pin_bytes = 0;
+      const size_t want = off[count] + off[count] / 4;
+      TAMC_CUDA(cudaHostAlloc((void**)&g->up_pin, want, cudaHostAllocDefault));
+      g->up_pin_bytes = want;
+    }
+    parallel([&](uint32_t k) { memcpy(g->up_pin + off[k], packs[k].host.data(), packs[k].host.size()); });
+    // device side in order: one allocation and one asynchronous copy per
+    // instance on the upload stream, then one wait for all of them (the
+    // instances are complete on return, as after tamc_gpu_instance_upload)
+    for (uint32_t k = 0; k < count; ++k) {
+      ds[k]->arena_bytes = packs[k].host.size();
+      ds[k]->arena = dev_alloc(ds[k]->arena_bytes);
+      TAMC_CUDA(copy_async(ds[k]->arena, g->up_pin + off[k], ds[k]->arena_bytes, cudaMemcpyHostToDevice,
+                           g->up_stream));
+      packs[k].bind(ds[k]->arena);
+    }
+    TAMC_CUDA(cudaStreamSynchronize(g->up_stream));
+  } catch (...) {
+    drop_all();
+    throw;
+  }
+  for (uint32_t k = 0; k < count; ++k) outs[k] = ds[k];
   TAMC_API_END
 }
 

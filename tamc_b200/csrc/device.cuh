@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -188,6 +189,12 @@ struct tamc_gpu {
   // reference; tamc_gpu_close only drops the caller's reference, so a
   // context is released after its last child whatever the destruction order.
   std::atomic<int> refs{1};
+  // bulk instance uploads: a pinned staging block (grows, kept for the next
+  // call) and a copy stream of their own, one bulk upload at a time
+  std::mutex up_mu;
+  cudaStream_t up_stream = nullptr;
+  char* up_pin = nullptr;
+  size_t up_pin_bytes = 0;
   void count(uint64_t k = 1) { launches.fetch_add(k, std::memory_order_relaxed); }
 };
 void tamc_gpu_retain(tamc_gpu* g);

@@ -1154,6 +1154,47 @@ int tamc_gpu_batch_gs(tamc_batch* b, uint32_t job, uint32_t cap, uint32_t* count
   return tamc_gpu_pt_gs(pt, cap, count, steps, energies, states);
   TAMC_API_END
 }
+int tamc_gpu_batch_gs_all(tamc_batch* b, uint64_t cap_entries, uint64_t cap_words, uint32_t* counts,
+                          uint32_t* steps, float* energies, uint64_t* states) {
+  TAMC_API_BEGIN
+  if (!b || !counts) fail(TAMC_E_INVAL, "null argument");
+  const uint32_t nj = (uint32_t)b->jobs.size();
+  uint64_t entries = 0, words = 0;
+  for (uint32_t j = 0; j < nj; ++j) {
+    const int rc = tamc_gpu_batch_gs(b, j, 0, &counts[j], nullptr, nullptr, nullptr);
+    if (rc != TAMC_OK) return rc;
+    entries += counts[j];
+    words += (uint64_t)counts[j] * ((b->jobs[j]->inst->n + 63) / 64);
+  }
+  if (!steps && !energies && !states) return TAMC_OK;
+  if (!steps || !energies || !states) fail(TAMC_E_INVAL, "steps, energies and states go together");
+  if (entries > cap_entries || words > cap_words)
+    fail(TAMC_E_INVAL, "output capacity below the logs' " + std::to_string(entries) + " entries / " +
+                           std::to_string(words) + " state words");
+  uint64_t eo = 0, wo = 0;
+  for (uint32_t j = 0; j < nj; ++j) {
+    uint32_t c = counts[j];
+    const int rc = tamc_gpu_pt_gs(b->jobs[j], c, &c, steps + eo, energies + eo, states + wo);
+    if (rc != TAMC_OK) return rc;
+    eo += counts[j];
+    wo += (uint64_t)counts[j] * ((b->jobs[j]->inst->n + 63) / 64);
+  }
+  TAMC_API_END
+}
+int tamc_gpu_batch_acceptance_all(tamc_batch* b, uint64_t cap, uint32_t* counts) {
+  TAMC_API_BEGIN
+  if (!b || !counts) fail(TAMC_E_INVAL, "null argument");
+  uint64_t need = 0;
+  for (tamc_pt* pt : b->jobs) need += pt->cfg.nt;
+  if (need > cap) fail(TAMC_E_INVAL, "output capacity below the " + std::to_string(need) + " counts of the batch");
+  uint64_t o = 0;
+  for (uint32_t j = 0; j < (uint32_t)b->jobs.size(); ++j) {
+    const int rc = tamc_gpu_batch_acceptance(b, j, counts + o);
+    if (rc != TAMC_OK) return rc;
+    o += b->jobs[j]->cfg.nt;
+  }
+  TAMC_API_END
+}
 int tamc_gpu_batch_samples_dims(tamc_batch* b, uint32_t job, uint32_t* M, uint32_t* S, uint32_t* Z, uint32_t* nchi) {
   TAMC_API_BEGIN
   return tamc_gpu_pt_samples_dims(job_of(b, job), M, S, Z, nchi);

@@ -270,12 +270,57 @@ def test_batch_equals_single_runs(tb, po, gpu):
         batch.add(d, p, 50 + k)
         singles.append(tb.PtRun(d, p, 50 + k).run().sync())
     batch.run()
+    ga, aa = batch.gs_all(), batch.acceptance_all()  # the batch-wide reads, first after the run
+    assert len(ga) == len(aa) == len(jobs)
     for k, r in enumerate(singles):
         S1, E1 = r.state()
         S2, E2 = batch.state(k)
         assert np.array_equal(S1, S2) and np.array_equal(E1, E2), k
         assert np.array_equal(r.gs()[1], batch.gs(k)[1])
         assert np.array_equal(r.acceptance(), batch.acceptance(k))
+        for x, y in zip(r.gs(), ga[k]):
+            assert np.array_equal(x, y), k
+        assert np.array_equal(aa[k], r.acceptance()), k
+
+
+def test_upload_many_equals_single_uploads(tb, po, gpu):
+    """Instances uploaded in one call (host preparation on several threads)
+    run exactly as instances uploaded one by one: a batch over lattices of
+    both dimensions, a periodic 2-D L=16 lattice (bitmap Houdayer layout), a
+    QUBO with diagonal terms and susceptibility weights gives the same states,
+    energies, ground-state logs and acceptance counts bit for bit.  A list
+    holding an instance without sites is refused, naming its index, and
+    returns nothing."""
+    texts = [(gi.lattice(8, 2, "pm", 1), False), (gi.lattice(6, 3, "gauss", 2), False),
+             (gi.lattice(16, 2, "pm", 3), False), (gi.qubo_er(40, 4.0, 4), True),
+             (gi.lattice(12, 2, "gauss", 5), False)]
+    hosts = []
+    for text, qubo in texts:
+        h = tb.HostInstance.parse(text, qubo=qubo)
+        h.add_suscept(np.linspace(-1.0, 1.0, h.n))
+        hosts.append(h)
+    one = [gpu.upload(h) for h in hosts]
+    many = gpu.upload_many(hosts)
+    assert [d.n for d in many] == [h.n for h in hosts]
+    out = []
+    for ds in (one, many):
+        batch = tb.Batch(gpu)
+        for k, d in enumerate(ds):
+            b = po.geometric_betas(0.2, 5.0, 16)
+            batch.add(d, tb.PtParams(60, b, po.lo_beta_idx(b, lo_beta=1.0), 0.5, True, 2, 4, 6, None, 0), 80 + k)
+        batch.run()
+        out.append([(batch.state(k), batch.gs(k)[1], batch.acceptance(k),
+                     np.array(batch.samples(k).suscept)) for k in range(len(ds))])
+    for k, (a, c) in enumerate(zip(*out)):
+        assert np.array_equal(a[0][0], c[0][0]) and np.array_equal(a[0][1], c[0][1]), k
+        for x, y in zip(a[1:], c[1:]):
+            assert np.array_equal(x, y), k
+    empty = tb.HostInstance.from_csr(np.zeros(1, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.float32),
+                                     np.zeros(0, np.float32))
+    with pytest.raises(tb.TamcError) as err:
+        gpu.upload_many([hosts[0], hosts[1], empty])
+    assert err.value.code == -1 and "index 2" in str(err.value)
+    assert gpu.upload_many([]) == []
 
 
 def test_batch_two_class_launch_identical_to_one_launch(tb, po, gpu, monkeypatch):
