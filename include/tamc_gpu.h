@@ -149,7 +149,9 @@ void tamc_copy_bytes(uint64_t* h2d, uint64_t* d2h);
 int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* h, tamc_inst** out);
 /* Uploads `count` instances at once, as `count` calls of
  * tamc_gpu_instance_upload would (outs[k] for his[k]), with the host-side
- * preparation (colouring, re-layouts) spread over up to 16 threads.  For
+ * preparation (colouring, re-layouts) spread over up to 16 threads and the
+ * copies staged through a pinned block of the context in rounds of at most
+ * 256 MiB (TAMC_UPLOAD_STAGE_BYTES; an instance larger than that goes alone).  For
  * callers that upload many instances together, such as the instances of one
  * batch or GLA's sub-instances, which the reference builds all before it runs
  * them (src/gla.rs:137-153).  All or nothing: on an error no instance is

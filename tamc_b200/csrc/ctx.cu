@@ -1,5 +1,6 @@
 // ctx.cu -- device contexts and device-resident instances.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -472,11 +473,10 @@ int tamc_gpu_instance_upload_many(tamc_gpu* g, uint32_t count, const tamc_host_i
     std::vector<size_t> off(count + 1, 0);
     std::vector<std::exception_ptr> errs(count);
     const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
-    const uint32_t nth = std::min({count, hw, 16u});
-    auto parallel = [&](auto&& f) {
-      std::atomic<uint32_t> next{0};
+    auto parallel = [&](uint32_t k0, uint32_t k1, auto&& f) {
+      std::atomic<uint32_t> next{k0};
       auto work = [&] {
-        for (uint32_t k; (k = next.fetch_add(1)) < count;) {
+        for (uint32_t k; (k = next.fetch_add(1)) < k1;) {
           try {
             f(k);
           } catch (...) {
@@ -485,36 +485,44 @@ int tamc_gpu_instance_upload_many(tamc_gpu* g, uint32_t count, const tamc_host_i
         }
       };
       std::vector<std::thread> pool;
-      for (uint32_t t = 1; t < nth; ++t) pool.emplace_back(work);
+      for (uint32_t t = 1; t < std::min({k1 - k0, hw, 16u}); ++t) pool.emplace_back(work);
       work();
       for (auto& th : pool) th.join();
-      for (auto& e : errs)
-        if (e) std::rethrow_exception(e);
+      for (uint32_t k = k0; k < k1; ++k)
+        if (errs[k]) std::rethrow_exception(errs[k]);
     };
-    parallel([&](uint32_t k) { inst_prepare(ds[k], his[k]->h, packs[k]); });
+    parallel(0, count, [&](uint32_t k) { inst_prepare(ds[k], his[k]->h, packs[k]); });
     for (uint32_t k = 0; k < count; ++k) off[k + 1] = off[k] + ((packs[k].host.size() + 255) & ~(size_t)255);
+    // staged in rounds of at most `cap` bytes (one instance at least): fill
+    // the block, one device allocation and one asynchronous copy per instance
+    // on the upload stream, one wait; the instances are complete on return,
+    // as after tamc_gpu_instance_upload
+    size_t cap = (size_t)256 << 20;
+    if (const char* e = getenv("TAMC_UPLOAD_STAGE_BYTES")) cap = std::max<size_t>(256, strtoull(e, nullptr, 10));
     std::lock_guard<std::mutex> lk(g->up_mu);
     if (!g->up_stream) TAMC_CUDA(cudaStreamCreateWithFlags(&g->up_stream, cudaStreamNonBlocking));
-    if (off[count] > g->up_pin_bytes) {
-      if (g->up_pin) TAMC_CUDA(cudaFreeHost(g->up_pin));
-      g->up_pin = nullptr;
-      g->up_pin_bytes = 0;
-      const size_t want = off[count] + off[count] / 4;
-      TAMC_CUDA(cudaHostAlloc((void**)&g->up_pin, want, cudaHostAllocDefault));
-      g->up_pin_bytes = want;
+    for (uint32_t k0 = 0, k1; k0 < count; k0 = k1) {
+      k1 = k0 + 1;
+      while (k1 < count && off[k1 + 1] - off[k0] <= cap) ++k1;
+      const size_t bytes = off[k1] - off[k0];
+      if (bytes > g->up_pin_bytes) {
+        if (g->up_pin) TAMC_CUDA(cudaFreeHost(g->up_pin));
+        g->up_pin = nullptr;
+        g->up_pin_bytes = 0;
+        const size_t want = bytes > cap ? bytes : std::min(cap, bytes + bytes / 4);
+        TAMC_CUDA(cudaHostAlloc((void**)&g->up_pin, want, cudaHostAllocDefault));
+        g->up_pin_bytes = want;
+      }
+      auto pin = [&](uint32_t k) { return g->up_pin + (off[k] - off[k0]); };
+      parallel(k0, k1, [&](uint32_t k) { memcpy(pin(k), packs[k].host.data(), packs[k].host.size()); });
+      for (uint32_t k = k0; k < k1; ++k) {
+        ds[k]->arena_bytes = packs[k].host.size();
+        ds[k]->arena = dev_alloc(ds[k]->arena_bytes);
+        TAMC_CUDA(copy_async(ds[k]->arena, pin(k), ds[k]->arena_bytes, cudaMemcpyHostToDevice, g->up_stream));
+        packs[k].bind(ds[k]->arena);
+      }
+      TAMC_CUDA(cudaStreamSynchronize(g->up_stream));
     }
-    parallel([&](uint32_t k) { memcpy(g->up_pin + off[k], packs[k].host.data(), packs[k].host.size()); });
-    // device side in order: one allocation and one asynchronous copy per
-    // instance on the upload stream, then one wait for all of them (the
-    // instances are complete on return, as after tamc_gpu_instance_upload)
-    for (uint32_t k = 0; k < count; ++k) {
-      ds[k]->arena_bytes = packs[k].host.size();
-      ds[k]->arena = dev_alloc(ds[k]->arena_bytes);
-      TAMC_CUDA(copy_async(ds[k]->arena, g->up_pin + off[k], ds[k]->arena_bytes, cudaMemcpyHostToDevice,
-                           g->up_stream));
-      packs[k].bind(ds[k]->arena);
-    }
-    TAMC_CUDA(cudaStreamSynchronize(g->up_stream));
   } catch (...) {
     drop_all();
     throw;

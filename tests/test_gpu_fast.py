@@ -283,14 +283,18 @@ def test_batch_equals_single_runs(tb, po, gpu):
         assert np.array_equal(aa[k], r.acceptance()), k
 
 
-def test_upload_many_equals_single_uploads(tb, po, gpu):
+@pytest.mark.parametrize("stage", [None, "40000"])
+def test_upload_many_equals_single_uploads(tb, po, gpu, monkeypatch, stage):
     """Instances uploaded in one call (host preparation on several threads)
     run exactly as instances uploaded one by one: a batch over lattices of
     both dimensions, a periodic 2-D L=16 lattice (bitmap Houdayer layout), a
     QUBO with diagonal terms and susceptibility weights gives the same states,
     energies, ground-state logs and acceptance counts bit for bit.  A list
     holding an instance without sites is refused, naming its index, and
-    returns nothing."""
+    returns nothing.  With a staging limit of 40 kB the instances go to the
+    device in several rounds, those larger than the limit alone."""
+    if stage:
+        monkeypatch.setenv("TAMC_UPLOAD_STAGE_BYTES", stage)
     texts = [(gi.lattice(8, 2, "pm", 1), False), (gi.lattice(6, 3, "gauss", 2), False),
              (gi.lattice(16, 2, "pm", 3), False), (gi.qubo_er(40, 4.0, 4), True),
              (gi.lattice(12, 2, "gauss", 5), False)]
