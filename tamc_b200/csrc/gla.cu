@@ -183,11 +183,15 @@ int tamc_gla_run(tamc_gpu* g, const tamc_host_instance* hi, const tamc_partition
       if (d) tamc_gpu_instance_destroy(d);
   };
   try {
+    // the sub-instances (induced_subgraph_instance_sorted, src/gla.rs:137-139),
+    // uploaded together
+    std::vector<tamc_host_instance> subs(np);
+    std::vector<const tamc_host_instance*> subp(np);
     for (uint32_t k = 0; k < np; ++k) {
-      tamc_host_instance sub;
-      sub.h = induced_sorted(h, sorted[k]);
-      check_rc(tamc_gpu_instance_upload(g, &sub, &dinst[k]));
+      subs[k].h = induced_sorted(h, sorted[k]);
+      subp[k] = &subs[k];
     }
+    check_rc(tamc_gpu_instance_upload_many(g, np, subp.data(), dinst.data()));
     if (mode == TAMC_MODE_REF) {
       // one master stream, cloned then jumped per sub-instance (src/gla.rs:144-151);
       // each clone draws its initial replicas, then runs the loop
