@@ -485,7 +485,13 @@ int tamc_gpu_instance_upload_many(tamc_gpu* g, uint32_t count, const tamc_host_i
         }
       };
       std::vector<std::thread> pool;
-      for (uint32_t t = 1; t < std::min({k1 - k0, hw, 16u}); ++t) pool.emplace_back(work);
+      for (uint32_t t = 1; t < std::min({k1 - k0, hw, 16u}); ++t) {
+        try {
+          pool.emplace_back(work);
+        } catch (...) {
+          break;  // no more threads: the ones running and this one share the work
+        }
+      }
       work();
       for (auto& th : pool) th.join();
       for (uint32_t k = k0; k < k1; ++k)
