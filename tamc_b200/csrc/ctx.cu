@@ -425,6 +425,7 @@ uint64_t tamc_gpu_launch_count(tamc_gpu* g) { return g ? g->launches.load() : 0;
 
 int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_inst** out) {
   TAMC_API_BEGIN
+  TraceRange tr("tamc upload");
   if (!g || !hi || !out) fail(TAMC_E_INVAL, "null argument");
   // an instance without sites has nothing to sample; refused here rather than
   // launching empty grids
@@ -448,6 +449,7 @@ int tamc_gpu_instance_upload(tamc_gpu* g, const tamc_host_instance* hi, tamc_ins
 int tamc_gpu_instance_upload_many(tamc_gpu* g, uint32_t count, const tamc_host_instance* const* his,
                                   tamc_inst** outs) {
   TAMC_API_BEGIN
+  TraceRange tr("tamc upload_many");
   if (!g || (count && (!his || !outs))) fail(TAMC_E_INVAL, "null argument");
   for (uint32_t k = 0; k < count; ++k) {
     if (!his[k]) fail(TAMC_E_INVAL, "null instance at index " + std::to_string(k));

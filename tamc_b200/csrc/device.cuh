@@ -9,6 +9,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "expf_exact.h"
 #include "internal.h"
 
@@ -38,6 +40,16 @@ inline cudaError_t copy_sync(void* dst, const void* src, size_t bytes, cudaMemcp
   count_copy(bytes, kind);
   return cudaMemcpy(dst, src, bytes, kind);
 }
+
+// A named NVTX range over a host-side scope (nvtx3, header-only: it costs a
+// few nanoseconds unless a profiler such as Nsight Systems is attached, which
+// then shows the library's uploads, runs and chunks on its timeline).
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
 
 // Device memory of the library's handles (on the current device).  Blocks up
 // to a few MiB come from a per-device cache of freed blocks in power-of-two

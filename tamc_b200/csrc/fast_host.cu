@@ -304,6 +304,7 @@ static void plain_enqueue_rounds(tamc_pt* pt, uint32_t K) {
 }
 
 static void plain_run_chunk(tamc_pt* pt, uint32_t K) {
+  TraceRange tr("tamc plain chunk");
   auto* F = pt->fast;
   cudaStream_t st = pt->g->stream;
   auto it = F->graphs.find(K);
@@ -963,6 +964,7 @@ struct ChunkRunner {
   void run_all(tamc_gpu* g, const std::vector<tamc_pt*>& jobs, uint32_t chunk) {
     uint32_t k = 0;
     for (;; k ^= 1) {
+      TraceRange tr("tamc batch chunk");
       Slot& sl = slots[k];
       finish(g, sl, true, 2);  // the chunk that used these buffers two chunks ago
       if (!enqueue(g, sl, jobs, chunk, true, false, true)) break;
@@ -1090,6 +1092,7 @@ int tamc_gpu_batch_add(tamc_batch* b, tamc_inst* inst, const tamc_pt_params* p, 
 
 int tamc_gpu_batch_run(tamc_batch* b) {
   TAMC_API_BEGIN
+  TraceRange tr("tamc batch run");
   if (!b) fail(TAMC_E_INVAL, "null batch");
   TAMC_CUDA(cudaSetDevice(b->g->device));
   b->runner->run_all(b->g, b->jobs, b->chunk);

@@ -290,6 +290,7 @@ int tamc_gpu_pt_create(tamc_inst* inst, const tamc_pt_params* p, uint64_t seed, 
 }
 
 int tamc_gpu_pt_run(tamc_pt* pt, uint32_t sweep_end) {
+  TraceRange tr("tamc pt run");
   TAMC_API_BEGIN
   if (!pt) fail(TAMC_E_INVAL, "null handle");
   TAMC_CUDA(cudaSetDevice(pt->g->device));

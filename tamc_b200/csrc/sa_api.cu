@@ -57,6 +57,7 @@ extern "C" {
 int tamc_gpu_sa_run(tamc_inst* inst, const float* betas, uint32_t nbeta, uint32_t num_replicas, uint32_t threads,
                     uint64_t seed, int mode, float* energies_out, uint8_t* packed_out, uint32_t* r_eff) {
   TAMC_API_BEGIN
+  TraceRange tr("tamc sa run");
   if (!inst || (nbeta && !betas)) fail(TAMC_E_INVAL, "null argument");
   if (threads == 0) fail(TAMC_E_REFPANIC, "threads must be >= 1 (the reference divides by it)");
   if (num_replicas == 0) fail(TAMC_E_INVAL, "num_replicas must be >= 1");

@@ -153,6 +153,7 @@ int tamc_serve_submit(tamc_server* s, const tamc_host_instance* inst, const tamc
 
 int tamc_serve_step(tamc_server* s, uint32_t* active, uint32_t* queued) {
   TAMC_API_BEGIN
+  TraceRange tr("tamc serve step");
   if (!s) fail(TAMC_E_INVAL, "null server");
   TAMC_CUDA(cudaSetDevice(s->g->device));
   // admission: FIFO while slots and HBM budget allow
