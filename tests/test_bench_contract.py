@@ -29,3 +29,21 @@ def test_reference_arm_prints_the_contract_line():
                            "d2h_bytes_per_step": 0}
     # the per-step time is the whole batch's flips at the measured rate
     assert abs(line["ms_per_step"] - bench.c3_flips(bench.c3_jobs()) / line["value"] * 1e3) < 1e-6 * line["ms_per_step"]
+
+
+def test_reference_arm_under_torchrun_prints_one_line_from_rank_0():
+    """Launched like the GPU arm on two ranks, the reference arm runs on rank
+    0 alone and prints one line; the other rank exits 0 without work."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl", "reference",
+           "--gpus", "2", "--steps", "1", "--warmup", "3", "--cpu-stride", "256"]
+    cp = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
+    assert cp.returncode == 0, cp.stderr[-2000:]
+    lines = [ln for ln in cp.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
