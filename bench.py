@@ -703,6 +703,7 @@ def workload_pt_c4(args, tb, gi, gpu, cpu=True):
     first, tts = _time_to_target(tb, d, p, 2, best, t_gpu / sweeps)
     out = {"workload": "pt_c4: 3-D L=16 Gaussian, 64 temperatures, 2 chains, ICM, samples every 32",
            "sweeps": sweeps, "flips": flips, "gpu_flips_per_s": flips / t_gpu, "gpu_s": t_gpu,
+           "round_us": t_gpu / sweeps * 1e6,
            "gpu_best_energy": best, "target_energy": best,
            "target_first_sweep": first, "time_to_target_s": tts}
     if cpu and not args.no_cpu:
