@@ -1070,6 +1070,8 @@ int tamc_gpu_batch_create(tamc_gpu* g, tamc_batch** out) {
   if (!g || !out) fail(TAMC_E_INVAL, "null argument");
   auto* b = new tamc_batch();
   b->g = g;
+  if (const char* e = getenv("TAMC_BATCH_CHUNK"))  // rounds per chunk launch (1..1024)
+    b->chunk = std::min(1024u, std::max(1u, (uint32_t)strtoul(e, nullptr, 10)));
   b->runner = runner_take(g);
   tamc_gpu_retain(g);
   *out = b;
